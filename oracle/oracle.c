@@ -1,0 +1,458 @@
+/*
+ * oracle.c -- CPU restatement of the reference's NTT / coset-LDE path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the parity checker and the timed CPU baseline.
+ * The product library never links or calls this file.  Each function cites
+ * the reference file:line it restates (paths inside the reference project).
+ */
+#include "oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ===================== BabyBear (src/field/babybear.rs) ================== */
+
+#define BB_P ORC_BB_P
+#define BB_R2 1172168163u        /* babybear.rs:25 R^2 mod p            */
+#define BB_MONTY_CONST 2013265919u /* babybear.rs:29 -p^-1 mod 2^32      */
+#define BB_ONE 268435454u        /* babybear.rs:22 R mod p (Montgomery 1) */
+#define BB_TWO_ADICITY 27u       /* babybear.rs:33                       */
+#define BB_ROOT_MONTY 1476048622u /* babybear.rs:37 (440564289 canonical) */
+
+uint32_t orc_bb_monty_reduce(uint64_t t) /* babybear.rs:41-51 */
+{
+    uint32_t t_lo = (uint32_t)t;
+    uint32_t m = t_lo * BB_MONTY_CONST;
+    uint64_t mp = (uint64_t)m * BB_P;
+    uint32_t r = (uint32_t)((t + mp) >> 32);
+    return r >= BB_P ? r - BB_P : r;
+}
+
+uint32_t orc_bb_to_monty(uint32_t v) { return orc_bb_monty_reduce((uint64_t)v * BB_R2); }
+uint32_t orc_bb_from_monty(uint32_t m) { return orc_bb_monty_reduce((uint64_t)m); }
+
+uint32_t orc_bb_add(uint32_t a, uint32_t b) /* babybear.rs:113-121 */
+{
+    uint32_t s = a + b;
+    return s >= BB_P ? s - BB_P : s;
+}
+
+uint32_t orc_bb_sub(uint32_t a, uint32_t b) /* babybear.rs:124-130 */
+{
+    return a >= b ? a - b : BB_P - (b - a);
+}
+
+uint32_t orc_bb_mul(uint32_t a, uint32_t b) /* babybear.rs:133-137 */
+{
+    return orc_bb_monty_reduce((uint64_t)a * b);
+}
+
+uint32_t orc_bb_reduce(uint64_t v) /* babybear.rs:140-145 */
+{
+    return orc_bb_to_monty((uint32_t)(v % BB_P));
+}
+
+uint32_t orc_bb_inv(uint32_t a) /* babybear.rs:147-161, Fermat a^(p-2) */
+{
+    uint32_t result = BB_ONE, base = a, e = BB_P - 2;
+    while (e > 0) {
+        if (e & 1) result = orc_bb_mul(result, base);
+        base = orc_bb_mul(base, base);
+        e >>= 1;
+    }
+    return result;
+}
+
+uint32_t orc_bb_two_adic_generator(uint32_t log_n) /* babybear.rs:69-76 */
+{
+    uint32_t g = BB_ROOT_MONTY;
+    for (uint32_t i = 0; i < BB_TWO_ADICITY - log_n; i++) g = orc_bb_mul(g, g);
+    return g;
+}
+
+/* ========================= M31 (src/field/m31.rs) ======================== */
+
+#define M31_P ORC_M31_P
+
+uint32_t orc_m31_reduce(uint64_t v) /* m31.rs:54-67 */
+{
+    uint32_t lo = (uint32_t)(v & 0x7FFFFFFFu);
+    uint32_t hi = (uint32_t)(v >> 31);
+    uint32_t s = lo + hi;
+    return s >= M31_P ? s - M31_P : s;
+}
+
+uint32_t orc_m31_add(uint32_t a, uint32_t b) { return orc_m31_reduce((uint64_t)a + b); }
+
+uint32_t orc_m31_sub(uint32_t a, uint32_t b) /* m31.rs:38-45 */
+{
+    return a >= b ? a - b : M31_P - (b - a);
+}
+
+uint32_t orc_m31_mul(uint32_t a, uint32_t b) { return orc_m31_reduce((uint64_t)a * b); }
+
+uint32_t orc_m31_inv(uint32_t a) /* m31.rs:69-83 */
+{
+    uint32_t result = 1, base = a, e = M31_P - 2;
+    while (e > 0) {
+        if (e & 1) result = orc_m31_mul(result, base);
+        base = orc_m31_mul(base, base);
+        e >>= 1;
+    }
+    return result;
+}
+
+/* ===================== Circle group (src/field/circle.rs) ================ */
+
+static const orc_cpoint CIRCLE_GEN = {2u, 1268011823u};   /* circle.rs:17-20 */
+static const orc_cpoint CIRCLE_IDENTITY = {1u, 0u};       /* circle.rs:26-29 */
+
+orc_cpoint orc_circle_add(orc_cpoint a, orc_cpoint b) /* circle.rs:34-40 */
+{
+    orc_cpoint r;
+    r.x = orc_m31_sub(orc_m31_mul(a.x, b.x), orc_m31_mul(a.y, b.y));
+    r.y = orc_m31_add(orc_m31_mul(a.x, b.y), orc_m31_mul(a.y, b.x));
+    return r;
+}
+
+orc_cpoint orc_circle_double(orc_cpoint a) /* circle.rs:53-60 */
+{
+    orc_cpoint r;
+    r.x = orc_m31_sub(orc_m31_mul(2u, orc_m31_mul(a.x, a.x)), 1u);
+    r.y = orc_m31_mul(2u, orc_m31_mul(a.x, a.y));
+    return r;
+}
+
+orc_cpoint orc_circle_mul_scalar(orc_cpoint a, uint32_t n) /* circle.rs:63-74 */
+{
+    orc_cpoint result = CIRCLE_IDENTITY, base = a;
+    while (n > 0) {
+        if (n & 1) result = orc_circle_add(result, base);
+        base = orc_circle_add(base, base);
+        n >>= 1;
+    }
+    return result;
+}
+
+orc_cpoint orc_circle_subgroup_gen(uint32_t log_size) /* circle.rs:78-85 */
+{
+    orc_cpoint p = CIRCLE_GEN;
+    for (uint32_t i = 0; i < 31u - log_size; i++) p = orc_circle_double(p);
+    return p;
+}
+
+typedef struct { orc_cpoint initial, step; uint32_t log_size; } coset_t;
+
+static coset_t coset_odds(uint32_t log_size) /* circle.rs:108-117 */
+{
+    coset_t c;
+    c.step = orc_circle_subgroup_gen(log_size);
+    c.initial = orc_circle_subgroup_gen(log_size + 1);
+    c.log_size = log_size;
+    return c;
+}
+
+static orc_cpoint coset_at(const coset_t *c, size_t i) /* circle.rs:136-138 */
+{
+    return orc_circle_add(c->initial, orc_circle_mul_scalar(c->step, (uint32_t)i));
+}
+
+static coset_t coset_double(const coset_t *c) /* circle.rs:143-150 */
+{
+    coset_t d;
+    d.initial = orc_circle_double(c->initial);
+    d.step = orc_circle_double(c->step);
+    d.log_size = c->log_size - 1;
+    return d;
+}
+
+static size_t bit_reverse_idx(size_t index, uint32_t log_size) /* m31/twiddles.rs:71-79 */
+{
+    uint32_t v = (uint32_t)index, r = 0;
+    for (uint32_t i = 0; i < log_size; i++) {
+        r = (r << 1) | (v & 1);
+        v >>= 1;
+    }
+    return r;
+}
+
+/* ============================ Twiddles =================================== */
+
+/* BabyBear::generate_twiddles (babybear.rs:83-97): layer s holds g_{s+1}^j,
+ * j < 2^s; generate_inverse_twiddles (babybear/twiddles.rs:13-19) inverts
+ * every entry. */
+void orc_bb_twiddles(uint32_t log_n, int inverse, uint32_t *out)
+{
+    for (uint32_t s = 0; s < log_n; s++) {
+        size_t half = (size_t)1 << s;
+        uint32_t g = orc_bb_two_adic_generator(s + 1);
+        uint32_t w = BB_ONE;
+        uint32_t *layer = out + (half - 1);
+        for (size_t j = 0; j < half; j++) {
+            layer[j] = inverse ? orc_bb_inv(w) : w;
+            w = orc_bb_mul(w, g);
+        }
+    }
+}
+
+/* generate_twiddles / generate_itwiddles (m31/twiddles.rs:19-68) on
+ * Coset::odds(log_n): layer l holds the x coordinate (y on the last layer)
+ * of the l-times-doubled coset at bit-reversed positions. */
+void orc_m31_twiddles(uint32_t log_n, int inverse, uint32_t *out)
+{
+    size_t n = (size_t)1 << log_n;
+    coset_t cur = coset_odds(log_n);
+    for (uint32_t layer = 0; layer < log_n; layer++) {
+        size_t half = ((size_t)1 << cur.log_size) / 2;
+        int last = (layer == log_n - 1);
+        uint32_t *dst = out + (n - (n >> layer));
+        for (size_t i = 0; i < half; i++) {
+            orc_cpoint p = coset_at(&cur, bit_reverse_idx(i, cur.log_size - 1));
+            uint32_t t = last ? p.y : p.x;
+            dst[i] = inverse ? orc_m31_inv(t) : t;
+        }
+        cur = coset_double(&cur);
+    }
+}
+
+/* TwiddleCache (src/ntt/twiddle_cache.rs): one cached table per
+ * (field, direction, log_n).  Tables are filled before any parallel region. */
+static uint32_t *g_tw_cache[2][2][32];
+
+static const uint32_t *tw_get(int field_m31, int inverse, uint32_t log_n)
+{
+    uint32_t **slot = &g_tw_cache[field_m31][inverse][log_n];
+    if (*slot == NULL) {
+        size_t n = (size_t)1 << log_n;
+        uint32_t *t = (uint32_t *)malloc(n * sizeof(uint32_t));
+        if (field_m31) orc_m31_twiddles(log_n, inverse, t);
+        else orc_bb_twiddles(log_n, inverse, t);
+        *slot = t;
+    }
+    return *slot;
+}
+
+static int is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
+static uint32_t ilog2(size_t n) { uint32_t l = 0; while (((size_t)1 << l) < n) l++; return l; }
+
+/* ====================== BabyBear NTT (cpu_reference.rs) ================== */
+
+static void bb_forward_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *tw)
+{
+    for (int layer = (int)log_n - 1; layer >= 0; layer--) { /* cpu_reference.rs:45-60 */
+        size_t half = (size_t)1 << layer, full = half << 1;
+        const uint32_t *t = tw + (half - 1);
+        for (size_t block = 0; block < n / full; block++) {
+            for (size_t j = 0; j < half; j++) {
+                size_t i0 = block * full + j, i1 = i0 + half;
+                uint32_t v0 = data[i0], v1 = data[i1];
+                data[i0] = orc_bb_add(v0, v1);
+                data[i1] = orc_bb_mul(orc_bb_sub(v0, v1), t[j]);
+            }
+        }
+    }
+}
+
+static void bb_inverse_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *itw,
+                          int normalize)
+{
+    for (uint32_t layer = 0; layer < log_n; layer++) { /* cpu_reference.rs:80-95 */
+        size_t half = (size_t)1 << layer, full = half << 1;
+        const uint32_t *t = itw + (half - 1);
+        for (size_t block = 0; block < n / full; block++) {
+            for (size_t j = 0; j < half; j++) {
+                size_t i0 = block * full + j, i1 = i0 + half;
+                uint32_t tmp = orc_bb_mul(data[i1], t[j]);
+                uint32_t v0 = data[i0];
+                data[i0] = orc_bb_add(v0, tmp);
+                data[i1] = orc_bb_sub(v0, tmp);
+            }
+        }
+    }
+    if (normalize) { /* cpu_reference.rs:97-101 */
+        uint32_t inv_n = orc_bb_inv(orc_bb_reduce(n));
+        for (size_t i = 0; i < n; i++) data[i] = orc_bb_mul(data[i], inv_n);
+    }
+}
+
+int orc_bb_forward(uint32_t *data, size_t n)
+{
+    if (!is_pow2(n)) return 1;
+    if (n == 1) return 0;
+    uint32_t log_n = ilog2(n);
+    if (log_n > BB_TWO_ADICITY) return 1;
+    bb_forward_tw(data, n, log_n, tw_get(0, 0, log_n));
+    return 0;
+}
+
+int orc_bb_inverse(uint32_t *data, size_t n)
+{
+    if (!is_pow2(n)) return 1;
+    if (n == 1) return 0;
+    uint32_t log_n = ilog2(n);
+    if (log_n > BB_TWO_ADICITY) return 1;
+    bb_inverse_tw(data, n, log_n, tw_get(0, 1, log_n), 1);
+    return 0;
+}
+
+/* ======================== M31 NTT (m31/cpu_reference.rs) ================= */
+
+static void m31_forward_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *tw)
+{
+    for (int layer = (int)log_n - 1; layer >= 0; layer--) { /* cpu_reference.rs:61-74 */
+        size_t half = (size_t)1 << layer, full = half << 1;
+        const uint32_t *t = tw + (n - (n >> layer));
+        for (size_t block = 0; block < n / full; block++) {
+            uint32_t w = t[block];
+            for (size_t j = 0; j < half; j++) {
+                size_t i0 = block * full + j, i1 = i0 + half;
+                uint32_t tmp = orc_m31_mul(data[i1], w); /* butterfly_forward :137-142 */
+                uint32_t v0 = data[i0];
+                data[i0] = orc_m31_add(v0, tmp);
+                data[i1] = orc_m31_sub(v0, tmp);
+            }
+        }
+    }
+}
+
+static void m31_inverse_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *itw)
+{
+    for (uint32_t layer = 0; layer < log_n; layer++) { /* cpu_reference.rs:93-107 */
+        size_t half = (size_t)1 << layer, full = half << 1;
+        const uint32_t *t = itw + (n - (n >> layer));
+        for (size_t block = 0; block < n / full; block++) {
+            uint32_t w = t[block];
+            for (size_t j = 0; j < half; j++) {
+                size_t i0 = block * full + j, i1 = i0 + half;
+                uint32_t v0 = data[i0], v1 = data[i1]; /* butterfly_inverse :148-153 */
+                data[i0] = orc_m31_add(v0, v1);
+                data[i1] = orc_m31_mul(orc_m31_sub(v0, v1), w);
+            }
+        }
+    }
+    uint32_t inv_n = orc_m31_inv(orc_m31_reduce(n)); /* cpu_reference.rs:113-117 */
+    for (size_t i = 0; i < n; i++) data[i] = orc_m31_mul(data[i], inv_n);
+}
+
+int orc_m31_forward(uint32_t *data, size_t n)
+{
+    if (!is_pow2(n)) return 1;
+    if (n == 1) return 0;
+    uint32_t log_n = ilog2(n);
+    if (log_n > 30) return 1;
+    m31_forward_tw(data, n, log_n, tw_get(1, 0, log_n));
+    return 0;
+}
+
+int orc_m31_inverse(uint32_t *data, size_t n)
+{
+    if (!is_pow2(n)) return 1;
+    if (n == 1) return 0;
+    uint32_t log_n = ilog2(n);
+    if (log_n > 30) return 1;
+    m31_inverse_tw(data, n, log_n, tw_get(1, 1, log_n));
+    return 0;
+}
+
+/* ============================ Batches ===================================== */
+
+static int clamp_threads(int threads) { return threads < 1 ? 1 : threads; }
+
+int orc_bb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    if (log_n > BB_TWO_ADICITY) return 1;
+    if (log_n == 0) return 0;
+    size_t n = (size_t)1 << log_n;
+    const uint32_t *tw = tw_get(0, 0, log_n);
+    long c;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
+    for (c = 0; c < (long)batch; c++) bb_forward_tw(data + (size_t)c * n, n, log_n, tw);
+    return 0;
+}
+
+int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    if (log_n > BB_TWO_ADICITY) return 1;
+    if (log_n == 0) return 0;
+    size_t n = (size_t)1 << log_n;
+    const uint32_t *itw = tw_get(0, 1, log_n);
+    long c;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
+    for (c = 0; c < (long)batch; c++) bb_inverse_tw(data + (size_t)c * n, n, log_n, itw, 1);
+    return 0;
+}
+
+/* ========================= Coset LDE (src/lde/mod.rs) ==================== */
+
+/* coset_lde_batch_cpu (lde/mod.rs:127-176): per-column inverse, zero-pad
+ * copy, coset shift over rows-then-columns with shift =
+ * two_adic_generator(log_n_ext + 1) (lde/mod.rs:158), per-column forward. */
+int orc_bb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                     uint32_t added_bits, uint32_t shift_monty, int threads)
+{
+    uint32_t log_n_ext = log_n + added_bits;
+    if (log_n_ext + 1 > BB_TWO_ADICITY) return 1;
+    size_t n = (size_t)1 << log_n, n_ext = (size_t)1 << log_n_ext;
+    uint32_t shift = shift_monty ? shift_monty : orc_bb_two_adic_generator(log_n_ext + 1);
+    const uint32_t *itw = log_n ? tw_get(0, 1, log_n) : NULL;
+    const uint32_t *tw = log_n_ext ? tw_get(0, 0, log_n_ext) : NULL;
+    long c;
+    (void)threads;
+
+    /* shift powers, shared by every column (the reference recomputes the
+     * running power in its row loop; the values are identical) */
+    uint32_t *pw = (uint32_t *)malloc(n_ext * sizeof(uint32_t));
+    uint32_t p = BB_ONE;
+    for (size_t i = 0; i < n_ext; i++) { pw[i] = p; p = orc_bb_mul(p, shift); }
+
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
+    for (c = 0; c < (long)batch; c++) {
+        uint32_t *dst = out + (size_t)c * n_ext;
+        memcpy(dst, in + (size_t)c * n, n * sizeof(uint32_t));          /* step 1+2 */
+        if (log_n) bb_inverse_tw(dst, n, log_n, itw, 1);
+        memset(dst + n, 0, (n_ext - n) * sizeof(uint32_t));
+        for (size_t i = 0; i < n_ext; i++) dst[i] = orc_bb_mul(dst[i], pw[i]); /* step 3 */
+        if (log_n_ext) bb_forward_tw(dst, n_ext, log_n_ext, tw);        /* step 4 */
+    }
+    free(pw);
+    return 0;
+}
+
+int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                uint32_t added_bits, int threads)
+{
+    uint32_t log_n_ext = log_n + added_bits;
+    if (log_n_ext > 30) return 1;
+    size_t n = (size_t)1 << log_n, n_ext = (size_t)1 << log_n_ext;
+    const uint32_t *itw = log_n ? tw_get(1, 1, log_n) : NULL;
+    const uint32_t *tw = log_n_ext ? tw_get(1, 0, log_n_ext) : NULL;
+    long c;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
+    for (c = 0; c < (long)batch; c++) {
+        uint32_t *dst = out + (size_t)c * n_ext;
+        memcpy(dst, in + (size_t)c * n, n * sizeof(uint32_t));
+        if (log_n) m31_inverse_tw(dst, n, log_n, itw);
+        memset(dst + n, 0, (n_ext - n) * sizeof(uint32_t));
+        if (log_n_ext) m31_forward_tw(dst, n_ext, log_n_ext, tw);
+    }
+    return 0;
+}
+
+/* ============================ Data generator ============================= */
+
+uint64_t orc_lcg_fill(uint32_t *out, size_t n, uint64_t seed, uint32_t p, int monty)
+{
+    uint64_t s = seed;
+    for (size_t i = 0; i < n; i++) {
+        s = s * 6364136223846793005ull + 1ull;
+        uint32_t v = (uint32_t)(s >> 33) % p;
+        out[i] = monty ? orc_bb_to_monty(v) : v;
+    }
+    return s;
+}

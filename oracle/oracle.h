@@ -1,0 +1,104 @@
+/*
+ * oracle.h -- CPU restatement of the reference's NTT / coset-LDE path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This code is the parity checker for the CUDA
+ * library (tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * reference legs are its only users).  It is never linked into, called by or
+ * shipped with the product library.
+ *
+ * It restates, in plain C, the pure-Rust CPU modules of
+ * moven0831/small-field-metal-ntt (a Rust crate that cannot be compiled here:
+ * no cargo/rustc in the image and it needs the macOS `metal` crate):
+ *
+ *   src/field/m31.rs:18-94            M31 (p = 2^31-1), canonical form
+ *   src/field/babybear.rs:14-172      BabyBear (p = 2^31-2^27+1), Montgomery form
+ *   src/field/circle.rs:10-151        circle group over M31, cosets
+ *   src/ntt/m31/twiddles.rs:19-79     Circle-NTT twiddles (x / y coordinates)
+ *   src/ntt/babybear/twiddles.rs:13-19 + babybear.rs:83-97  BabyBear twiddles
+ *   src/ntt/m31/cpu_reference.rs:50-153       DCCT forward / inverse
+ *   src/ntt/babybear/cpu_reference.rs:34-103  GS-DIF forward / CT-DIT inverse
+ *   src/lde/mod.rs:116-176            coset_lde_batch_cpu
+ *
+ * Every function keeps the reference's loop structure (layer -> block -> j)
+ * so that it can also serve as the timed CPU baseline.
+ */
+#ifndef SFNTT_ORACLE_H
+#define SFNTT_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_BB_P 2013265921u          /* 0x78000001 */
+#define ORC_M31_P 2147483647u         /* 2^31 - 1   */
+
+/* ---- BabyBear field (src/field/babybear.rs) ---------------------------- */
+uint32_t orc_bb_monty_reduce(uint64_t t);        /* babybear.rs:41-51 */
+uint32_t orc_bb_to_monty(uint32_t v);            /* babybear.rs:54-59 */
+uint32_t orc_bb_from_monty(uint32_t m);          /* babybear.rs:62-65 */
+uint32_t orc_bb_add(uint32_t a, uint32_t b);     /* babybear.rs:113-121 */
+uint32_t orc_bb_sub(uint32_t a, uint32_t b);     /* babybear.rs:124-130 */
+uint32_t orc_bb_mul(uint32_t a, uint32_t b);     /* babybear.rs:133-137 */
+uint32_t orc_bb_reduce(uint64_t v);              /* babybear.rs:140-145 */
+uint32_t orc_bb_inv(uint32_t a);                 /* babybear.rs:147-161 */
+uint32_t orc_bb_two_adic_generator(uint32_t log_n); /* babybear.rs:69-76 */
+
+/* ---- M31 field (src/field/m31.rs) -------------------------------------- */
+uint32_t orc_m31_reduce(uint64_t v);             /* m31.rs:54-67 */
+uint32_t orc_m31_add(uint32_t a, uint32_t b);    /* m31.rs:32-35 */
+uint32_t orc_m31_sub(uint32_t a, uint32_t b);    /* m31.rs:38-45 */
+uint32_t orc_m31_mul(uint32_t a, uint32_t b);    /* m31.rs:48-51 */
+uint32_t orc_m31_inv(uint32_t a);                /* m31.rs:69-83 */
+
+/* ---- Circle group (src/field/circle.rs) -------------------------------- */
+typedef struct { uint32_t x, y; } orc_cpoint;
+orc_cpoint orc_circle_add(orc_cpoint a, orc_cpoint b);       /* circle.rs:34-40 */
+orc_cpoint orc_circle_double(orc_cpoint a);                  /* circle.rs:53-60 */
+orc_cpoint orc_circle_mul_scalar(orc_cpoint a, uint32_t n);  /* circle.rs:63-74 */
+orc_cpoint orc_circle_subgroup_gen(uint32_t log_size);       /* circle.rs:78-85 */
+
+/* ---- Twiddle tables ----------------------------------------------------
+ * Layers are concatenated: BabyBear layer s (2^s entries) starts at 2^s - 1;
+ * M31 layer l (n / 2^(l+1) entries) starts at n - n / 2^l.  Both total n - 1.
+ */
+void orc_bb_twiddles(uint32_t log_n, int inverse, uint32_t *out);  /* Montgomery form */
+void orc_m31_twiddles(uint32_t log_n, int inverse, uint32_t *out);
+
+/* ---- NTTs (in place; return 0, or 1 = InvalidSize) ---------------------- */
+int orc_bb_forward(uint32_t *data, size_t n);     /* cpu_reference.rs:34-62 */
+int orc_bb_inverse(uint32_t *data, size_t n);     /* cpu_reference.rs:69-103 */
+int orc_m31_forward(uint32_t *data, size_t n);    /* m31/cpu_reference.rs:50-79 */
+int orc_m31_inverse(uint32_t *data, size_t n);    /* m31/cpu_reference.rs:82-120 */
+
+/* ---- Coset LDE (src/lde/mod.rs:127-176) ---------------------------------
+ * in: batch columns of n = 2^log_n Montgomery u32 (SoA, in[col*n+row]).
+ * out: batch columns of 2^(log_n+added_bits).  shift_monty = 0 selects the
+ * reference default shift two_adic_generator(log_n + added_bits + 1).
+ * threads > 1 runs columns in parallel (OpenMP); the arithmetic is the same.
+ */
+int orc_bb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
+                     uint32_t batch, uint32_t added_bits, uint32_t shift_monty,
+                     int threads);
+
+/* M31 "LDE" used by the mixed-field batch / serving configurations: the
+ * reference has no M31 LDE, so it is defined as the composition of reference
+ * functions inverse(odds(log_n)) -> zero-pad -> forward(odds(log_n+added)). */
+int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
+                uint32_t batch, uint32_t added_bits, int threads);
+
+/* Column-parallel batched NTTs (used for the all-cores CPU baseline). */
+int orc_bb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
+int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
+
+/* Reference data generator (src/ntt/test_utils.rs:38-46, benches seeds):
+ * s = s*6364136223846793005 + 1; v = (s >> 33) % p.  to_monty applied when
+ * monty != 0.  Returns the final state. */
+uint64_t orc_lcg_fill(uint32_t *out, size_t n, uint64_t seed, uint32_t p, int monty);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

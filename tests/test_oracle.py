@@ -1,0 +1,243 @@
+"""Pins the C oracle (oracle/oracle.c) before any GPU result is compared to it.
+
+Known answers come from the reference's own tests:
+  tests/field_vectors.rs:16-182, src/field/babybear.rs:378-568,
+  src/field/m31.rs:144-203, src/field/circle.rs:153-235,
+  tests/ntt_cross_validation.rs:113-376, src/ntt/*/cpu_reference.rs tests,
+  src/lde/mod.rs:194-271.
+Fixtures come from tests/golden/gen_golden.py, an independent pure-Python
+restatement that checks itself against naive DFT / coset-evaluation closed forms.
+"""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+P = O.BB_P
+MP = O.M31_P
+
+
+def modpow(b, e, m):
+    return pow(b, e, m)
+
+
+def sha(a) -> str:
+    return hashlib.sha256(np.asarray(a, dtype="<u4").tobytes()).hexdigest()
+
+
+# ---- BabyBear KATs (tests/field_vectors.rs:15-116) ---------------------------
+def test_bb_modulus_and_constants():
+    assert P == (1 << 31) - (1 << 27) + 1
+    assert O.bb_to_monty(1) == (1 << 32) % P == 0x0FFFFFFE
+    assert O.bb_from_monty(O.bb_to_monty(1)) == 1
+    assert O.bb_to_monty(0) == 0
+    assert (P * 0x77FFFFFF + 1) % (1 << 32) == 0  # babybear.rs:561-568
+    assert O.bb_from_monty(1476048622) == 440564289  # babybear.rs:35-37
+
+
+def test_bb_arithmetic_kats():
+    a, b = O.bb_to_monty(123), O.bb_to_monty(456)
+    assert O.bb_from_monty(O.bb_mul(a, b)) == 56088
+    pm1 = O.bb_to_monty(P - 1)
+    assert O.bb_from_monty(O.bb_mul(pm1, pm1)) == 1
+    assert O.bb_from_monty(O.bb_add(pm1, O.bb_to_monty(1))) == 0
+    assert O.bb_from_monty(O.bb_sub(0, O.bb_to_monty(1))) == P - 1
+    for v in (0, 1, 2, 42, 1000, P - 1, P - 2):
+        assert O.bb_from_monty(O.bb_to_monty(v)) == v
+    assert O.bb_from_monty(O.bb_reduce(21)) == 21
+    assert O.bb_from_monty(O.bb_reduce(P + 5)) == 5
+    one = O.bb_to_monty(1)
+    assert O.bb_monty_reduce(one * one) == one
+
+
+def test_bb_inverse_kats():
+    seven = O.bb_to_monty(7)
+    inv7 = O.bb_inv(seven)
+    assert O.bb_from_monty(O.bb_mul(seven, inv7)) == 1
+    assert O.bb_from_monty(inv7) == modpow(7, P - 2, P)
+    assert O.bb_from_monty(O.bb_inv(O.bb_to_monty(1))) == 1
+    assert O.bb_from_monty(O.bb_inv(O.bb_to_monty(P - 1))) == P - 1
+    for v in (1, 2, 7, 100, 999999, P - 1, 42):
+        a = O.bb_to_monty(v)
+        assert O.bb_from_monty(O.bb_mul(a, O.bb_inv(a))) == 1
+
+
+def test_bb_root_orders():
+    one = O.bb_to_monty(1)
+    for k in range(1, 28):
+        g = O.bb_two_adic_generator(k)
+        v = g
+        for _ in range(k):
+            v = O.bb_mul(v, v)
+        assert v == one
+        v = g
+        for _ in range(k - 1):
+            v = O.bb_mul(v, v)
+        assert v != one
+    pm1, c = P - 1, 0
+    while pm1 % 2 == 0:
+        pm1 //= 2
+        c += 1
+    assert (c, pm1) == (27, 15)
+
+
+# ---- M31 / circle KATs (tests/field_vectors.rs:118-182, circle.rs tests) ----
+def test_m31_kats():
+    assert MP == 2147483647
+    assert O.m31_mul(123, 456) == 56088
+    assert O.m31_mul(MP - 1, MP - 1) == 1
+    assert O.m31_add(MP - 1, 1) == 0
+    assert O.m31_add(MP - 1, MP - 1) == MP - 2
+    assert O.m31_sub(0, 1) == MP - 1
+    assert O.m31_sub(8, 3) == 5
+    inv7 = O.m31_inv(7)
+    assert O.m31_mul(7, inv7) == 1 and inv7 == modpow(7, MP - 2, MP)
+    assert O.m31_inv(1) == 1 and O.m31_inv(MP - 1) == MP - 1
+    assert O.m31_reduce(0) == 0 and O.m31_reduce(MP) == 0
+    assert O.m31_mul(42, O.m31_inv(42)) == 1
+
+
+def test_circle_generator():
+    L = O.lib()
+    g = L.orc_circle_subgroup_gen(31)
+    assert (g.x, g.y) == (2, 1268011823)
+    assert O.m31_add(O.m31_mul(g.x, g.x), O.m31_mul(g.y, g.y)) == 1
+    p = g
+    for _ in range(30):
+        p = L.orc_circle_double(p)
+    assert (p.x, p.y) != (1, 0)
+    p = L.orc_circle_double(p)
+    assert (p.x, p.y) == (1, 0)
+    d, a = L.orc_circle_double(g), L.orc_circle_add(g, g)
+    assert (d.x, d.y) == (a.x, a.y)
+
+
+# ---- NTT KATs and structural tests -------------------------------------------
+def test_bb_polynomial_multiplication():  # ntt_cross_validation.rs:113-148
+    a = O.bb_forward([O.bb_to_monty(1), O.bb_to_monty(2), 0, 0])
+    b = O.bb_forward([O.bb_to_monty(3), O.bb_to_monty(4), 0, 0])
+    c = O.bb_inverse([O.bb_mul(int(x), int(y)) for x, y in zip(a, b)])
+    assert [O.bb_from_monty(int(v)) for v in c] == [3, 10, 8, 0]
+
+
+def _naive_dft_bitrev(x):
+    n = len(x)
+    log_n = n.bit_length() - 1
+    w = O.bb_from_monty(O.bb_two_adic_generator(log_n))
+    nat = [sum(int(x[i]) * pow(w, i * k, P) for i in range(n)) % P for k in range(n)]
+    rev = [int(format(k, f"0{log_n}b")[::-1], 2) for k in range(n)]
+    return [nat[r] for r in rev]
+
+
+@pytest.mark.parametrize("log_n", [2, 3, 4, 8, 10])
+def test_bb_forward_matches_plonky3_property(log_n):  # ntt_cross_validation.rs:43-110
+    n = 1 << log_n
+    x = [(i * 7 + 3) % P for i in range(n)]
+    got = O.bb_from_monty_array(O.bb_forward(O.bb_to_monty_array(x)))
+    assert list(got) == _naive_dft_bitrev(x)
+
+
+def test_bb_inverse_of_plonky3_forward():  # ntt_cross_validation.rs:151-182
+    vals = list(range(1, 17))
+    ev = _naive_dft_bitrev(vals)
+    got = O.bb_from_monty_array(O.bb_inverse(O.bb_to_monty_array(ev)))
+    assert list(got) == vals
+
+
+def test_m31_constant_and_zero_polys():  # ntt_cross_validation.rs:347-376
+    assert list(O.m31_forward([1, 0, 0, 0])) == [1, 1, 1, 1]
+    x = np.zeros(16, np.uint32)
+    x[0] = 1
+    assert np.all(O.m31_forward(x) == 1)
+    for log_n in range(1, 9):
+        assert not O.m31_forward(np.zeros(1 << log_n, np.uint32)).any()
+
+
+def test_m31_linearity_and_roundtrip():  # ntt_cross_validation.rs:300-344
+    n = 16
+    a = np.array([i + 1 for i in range(n)], np.uint32)
+    b = np.array([i * 3 + 2 for i in range(n)], np.uint32)
+    fa, fb = O.m31_forward(a), O.m31_forward(b)
+    fab = O.m31_forward([O.m31_add(int(x), int(y)) for x, y in zip(a, b)])
+    assert list(fab) == [O.m31_add(int(x), int(y)) for x, y in zip(fa, fb)]
+    for log_n in range(1, 13):
+        n = 1 << log_n
+        x = O.lcg(n, n * 11111 + 98765, MP)
+        f = O.m31_forward(x)
+        assert not np.array_equal(f, x)
+        assert np.array_equal(O.m31_inverse(f), x)
+
+
+def test_bb_linearity_roundtrip_edges():  # babybear/cpu_reference.rs:196-297
+    n = 16
+    a = O.bb_to_monty_array([i + 1 for i in range(n)])
+    b = O.bb_to_monty_array([i * 3 + 2 for i in range(n)])
+    fab = O.bb_forward([O.bb_add(int(x), int(y)) for x, y in zip(a, b)])
+    fa, fb = O.bb_forward(a), O.bb_forward(b)
+    assert list(fab) == [O.bb_add(int(x), int(y)) for x, y in zip(fa, fb)]
+    for n in (4, 256, 1024, 4096):
+        x = O.lcg(n, 12345 + n, P, monty=True)
+        assert np.array_equal(O.bb_inverse(O.bb_forward(x)), x)
+    assert not O.bb_forward(np.zeros(16, np.uint32)).any()
+    assert list(O.bb_forward([O.bb_to_monty(42)])) == [O.bb_to_monty(42)]
+    for bad in ([], [1, 2, 3]):
+        with pytest.raises(O.InvalidSize):
+            O.bb_forward(bad)
+        with pytest.raises(O.InvalidSize):
+            O.m31_inverse(bad)
+
+
+def test_bb_twiddle_inverses():  # babybear/twiddles.rs:32-75
+    fwd, inv = O.bb_twiddles(4), O.bb_twiddles(4, inverse=True)
+    one = O.bb_to_monty(1)
+    assert all(O.bb_mul(int(f), int(i)) == one for f, i in zip(fwd, inv))
+    assert fwd[0] == one and fwd[1] == one and fwd[3] == one
+
+
+# ---- oracle vs the independent restatement's fixtures -----------------------
+def test_oracle_matches_golden_ntts(golden):
+    meta, arr = golden
+    fns = {"bb_forward": O.bb_forward, "bb_inverse": O.bb_inverse,
+           "m31_forward": O.m31_forward, "m31_inverse": O.m31_inverse}
+    for key, fn in fns.items():
+        assert meta[key]
+        for case in meta[key]:
+            got = fn(arr[case["input"]])
+            assert np.array_equal(got, arr[case["output"]]), (key, case["log_n"])
+
+
+def test_oracle_matches_golden_twiddles(golden):
+    meta, _ = golden
+    for case in meta["bb_twiddles"]:
+        t = O.bb_twiddles(case["log_n"], case["inverse"])
+        assert sha(t) == case["sha256"] and list(t[:16]) == case["head"]
+    for case in meta["m31_twiddles"]:
+        t = O.m31_twiddles(case["log_n"], case["inverse"])
+        assert sha(t) == case["sha256"] and list(t[:16]) == case["head"]
+
+
+def test_oracle_matches_golden_lde(golden):
+    meta, arr = golden
+    for case in meta["bb_lde"]:
+        ln, b, ab = case["log_n"], case["batch"], case["added_bits"]
+        inp = O.lcg(b << ln, case["seed"], P, monty=True)
+        if "input" in case:
+            assert np.array_equal(inp, arr[case["input"]])
+        out = O.bb_coset_lde(inp, ln, b, ab, case.get("shift_monty", 0))
+        assert sha(out) == case["sha256"], case
+        par = O.bb_coset_lde(inp, ln, b, ab, case.get("shift_monty", 0), threads=4)
+        assert np.array_equal(out, par)
+    for case in meta["m31_lde"]:
+        ln, b, ab = case["log_n"], case["batch"], case["added_bits"]
+        out = O.m31_lde(arr[case["input"]], ln, b, ab)
+        assert np.array_equal(out, arr[case["output"]])
+
+
+def test_reference_lde_shift_default():
+    # lde/mod.rs:59, :158 -- shift = two_adic_generator(log_n_ext + 1)
+    assert O.bb_from_monty(O.bb_two_adic_generator(22)) == 570250684
+    assert O.bb_from_monty(O.bb_two_adic_generator(23)) == 1267047229
