@@ -1,0 +1,353 @@
+#!/usr/bin/env python3
+"""Benchmark of the BabyBear coset LDE, 2^20 rows x 256 columns, 2x blow-up.
+
+This is the reference's headline number (README.md:58: 821 ms on an Apple M3
+GPU, timed commit -> wait).  One step = one full LDE of 256 columns
+(iDFT -> n^-1 -> zero-pad -> coset shift -> DFT), inputs resident in HBM:
+1 GiB in, 2 GiB out, so every step streams more than the 126 MB L2.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU runs (torchrun, one rank per GPU) are weak-scaled replicas: every
+rank runs its own 256-column LDE with no data-path collective; `value` is the
+job's time per LDE (slowest rank's step time / N).
+
+`--impl reference` times the reference's CPU implementation of the path (the
+C restatement in oracle/, all host threads, a bounded sample of columns per
+step scaled to 256 columns).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "small-field-metal-ntt_b200"))
+sys.path.insert(0, str(ROOT))
+
+BB_P = 2013265921
+METRIC = "BabyBear coset LDE 2^20x256 2x"
+PUBLISHED_MS = 821.0  # BASELINE.md / README.md:58 (Apple M3, Metal)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--log-n", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--added-bits", type=int, default=1)
+    ap.add_argument("--mode", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a) -> dict:
+    return {"workload": f"BabyBear coset LDE 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x blow-up",
+            "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
+            "shift": "two_adic_generator(log_n_ext+1) (reference default)",
+            "layout": "SoA column-major, Montgomery u32",
+            "l2": "inputs larger than L2 (1 GiB in, 2 GiB out per step)"}
+
+
+def algorithmic_bytes(a) -> int:
+    return 4 * a.batch * (1 << a.log_n) * (1 + (1 << a.added_bits))
+
+
+# ----------------------------------------------------------------- clocks ---
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) during the timed region."""
+
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.proc = None
+        self.lines: list[str] = []
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self, t0: float, t1: float) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [l for (ts, l) in self.lines if t0 - 0.05 <= ts <= t1 + 0.1]
+        if not rows:
+            rows = [l for (_, l) in self.lines]
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            parts = [p.strip() for p in r.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+def peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if kernel in d:
+            return d[kernel]
+    return None
+
+
+# ------------------------------------------------------------ CPU legs ---
+def cpu_lde_sample(a, target_s: float) -> dict:
+    """The oracle (reference CPU path restated in C) on a bounded column
+    sample, all host threads; returns ms scaled to the full column count."""
+    from oracle import oracle as O
+    threads = O.default_threads()
+    n = 1 << a.log_n
+    one = O.lcg(n, 1, BB_P, monty=True)
+    t = time.perf_counter()
+    O.bb_coset_lde(one, a.log_n, 1, a.added_bits, threads=1)
+    t1 = time.perf_counter() - t
+    cols = int(max(1, min(a.batch, round(target_s * threads / max(t1, 1e-6)))))
+    cols = max(1, min(a.batch, (cols // threads) * threads or cols))
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
+    t = time.perf_counter()
+    O.bb_coset_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+    ts = time.perf_counter() - t
+    return {"value": ts * 1e3 * a.batch / cols, "unit": "ms", "cores": threads, "kind": "port",
+            "sample": f"{cols} of {a.batch} columns (oracle/oracle.c coset_lde, OpenMP over columns), "
+                      f"scaled x{a.batch / cols:.2f}; 1-thread column time {t1 * 1e3:.1f} ms",
+            "single_thread_ms_full": t1 * 1e3 * a.batch}
+
+
+def run_reference(a, rank: int) -> None:
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    threads = O.default_threads()
+    n = 1 << a.log_n
+    per_step = max(0.3, min(20.0, 150.0 / max(1, a.steps + a.warmup)))  # whole run ~2.5 min
+    t = time.perf_counter()
+    O.bb_coset_lde(O.lcg(n, 1, BB_P, monty=True), a.log_n, 1, a.added_bits, threads=1)
+    t1 = time.perf_counter() - t
+    cols = int(max(1, min(a.batch, round(per_step * threads / max(t1, 1e-6)))))
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
+    times = []
+    for i in range(a.warmup + a.steps):
+        t = time.perf_counter()
+        O.bb_coset_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+        if i >= a.warmup:
+            times.append((time.perf_counter() - t) * a.batch / cols)
+    ms = statistics.mean(times) * 1e3
+    sample = f"{cols} of {a.batch} columns per step (oracle/oracle.c, OpenMP over columns), scaled x{a.batch / cols:.2f}"
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": ms / PUBLISHED_MS, "dtype": "u32 (BabyBear Montgomery)", "data": "synthetic",
+            "config": workload(a),
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU leg ---
+def main() -> None:
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import sfntt
+
+    torch.cuda.set_device(local)
+    dist_on = world > 1
+    if dist_on:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist_on:
+            dist.barrier()
+
+    def max_all(v: float) -> float:
+        if not dist_on:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = sfntt.Context(local)
+    lde = sfntt.CosetLdeBatch(ctx, fused=(a.mode == "fused"))
+    n, n_ext = 1 << a.log_n, 1 << (a.log_n + a.added_bits)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    x = torch.randint(0, BB_P, (a.batch * n,), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    out = torch.empty(a.batch * n_ext, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
+    ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, 0)
+
+    def step():
+        lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    sampler = ClockSampler(gpu_id)
+    time.sleep(0.6)
+    ctx.kernel_timing(True)
+    launches0 = ctx.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    w1 = time.time()
+    barrier()
+    launches = ctx.launch_count() - launches0
+    kt = ctx.kernel_times()
+    ctx.kernel_timing(False)
+    clocks = sampler.stop(w0, w1)
+    step_ms = max_all(ev0.elapsed_time(ev1) / a.steps)
+    value = step_ms / world
+
+    # dominant kernel and its roofline
+    peak, peak_kind = peaks()
+    dom = max(kt.items(), key=lambda kv: kv[1][1])
+    name, (nl, tot_ms, nbytes) = dom
+    avg_ms = tot_ms / nl
+    achieved = (nbytes / nl) / (avg_ms * 1e-3) / 1e9
+    traffic = ncu_traffic(name)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": name, "kernel_ms": avg_ms,
+                "algorithmic_bytes_per_launch": nbytes // nl, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    kernels = {k: {"launches": v[0], "avg_ms": v[1] / v[0], "share": v[1] / sum(t[1] for t in kt.values()),
+                   "gbs": (v[2] / v[0]) / (v[1] / v[0] * 1e-3) / 1e9} for k, v in kt.items()}
+    lde_gbs = algorithmic_bytes(a) / (step_ms * 1e-3) / 1e9
+
+    # end to end through the host-buffer C-ABI call (copies inside the timed region)
+    e2e = None
+    if not a.no_e2e:
+        hin = ctx.pinned(a.batch * n)
+        hout = ctx.pinned(a.batch * n_ext)
+        hin.array[:] = x.cpu().numpy().view("uint32")
+        lde.execute(hin.array, a.log_n, a.batch, a.added_bits, out=hout.array)  # warm-up
+        barrier()
+        ts = []
+        for _ in range(a.e2e_steps):
+            t = time.perf_counter()
+            lde.execute(hin.array, a.log_n, a.batch, a.added_bits, out=hout.array)
+            ts.append(time.perf_counter() - t)
+        e2e_ms = max_all(statistics.mean(ts) * 1e3)
+        ok = bool((hout.array[: n_ext] == out[: n_ext].cpu().numpy().view("uint32")).all())
+        e2e = {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": 4 * a.batch * n,
+               "d2h_bytes_per_step": 4 * a.batch * n_ext, "steps": a.e2e_steps,
+               "path": "sfntt_bb_coset_lde (pinned host buffers, column chunks pipelined over 3 streams)",
+               "matches_device_run": ok}
+        hin.free()
+        hout.free()
+
+    secondary = secondary_metrics(ctx, sfntt, torch)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_lde_sample(a, a.cpu_seconds)
+
+    if dist_on:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_MS, "dtype": "u32 (BabyBear Montgomery, exact)",
+            "data": "synthetic: seeded uniform canonical values in [0, p), Montgomery on device",
+            "config": {**workload(a), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "gpu_launches": launches, "launches_per_step": launches / a.steps,
+            "lde_gbs": lde_gbs, "lde_hbm_frac": lde_gbs / peak,
+            "melem_per_s_out": a.batch * n_ext / (value * 1e-3) / 1e6,
+            "roofline": roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "secondary": secondary, "device": ctx.device_info()}
+    print(json.dumps(line), flush=True)
+
+
+def secondary_metrics(ctx, sfntt, torch) -> dict:
+    """The other two parts of the headline metric string: single-column NTT
+    throughput (Gelem/s) and the M31 2^16 forward+inverse pair."""
+    res = {}
+    stream = torch.cuda.current_stream().cuda_stream
+    for field, name, sizes in ((sfntt.FIELD_BABYBEAR, "bb", (16, 20, 24)), (sfntt.FIELD_M31, "m31", (16, 20))):
+        b = (sfntt.BbCudaCtGsR4 if field == sfntt.FIELD_BABYBEAR else sfntt.CudaCtGsR4)(ctx)
+        for log_n in sizes:
+            p = BB_P if field == sfntt.FIELD_BABYBEAR else 2147483647
+            d = torch.randint(0, p, (1 << log_n,), dtype=torch.int64, device="cuda").to(torch.int32)
+            ctx.prepare(field, log_n)
+            for _ in range(5):
+                b.forward_dev(d.data_ptr(), log_n, 1, stream)
+                b.inverse_dev(d.data_ptr(), log_n, 1, stream)
+            reps = 50
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                b.forward_dev(d.data_ptr(), log_n, 1, stream)
+                b.inverse_dev(d.data_ptr(), log_n, 1, stream)
+            e1.record()
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) * 1e3 / reps
+            res[f"{name}_fwd_inv_2^{log_n}_us"] = us
+            res[f"{name}_ntt_2^{log_n}_gelem_s"] = 2 * (1 << log_n) / (us * 1e-6) / 1e9
+    return res
+
+
+if __name__ == "__main__":
+    main()

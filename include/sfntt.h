@@ -1,0 +1,161 @@
+/*
+ * sfntt.h -- C ABI of the B200 (sm_100a) small-field NTT / coset-LDE library.
+ *
+ * Drop-in boundary for the NTT hot path of moven0831/small-field-metal-ntt.
+ * The reference is a Rust crate; a Rust FFI crate (sfntt-sys) binds these
+ * symbols one to one.  All functions are plain C:
+ * pointers, sizes and integer status codes, no C++ or torch types.
+ *
+ * Conventions (same as the reference):
+ *   - BabyBear values are Montgomery-form u32 in [0, p), p = 2^31 - 2^27 + 1
+ *     (src/field/babybear.rs:14-65).  M31 values are canonical u32 in [0, p),
+ *     p = 2^31 - 1 (src/field/m31.rs:18-67).
+ *   - Forward NTT: natural-order input, bit-reversed-order output.  Inverse:
+ *     bit-reversed input, natural output, multiplied by n^-1
+ *     (src/ntt/babybear/cpu_reference.rs:29-103, src/ntt/m31/cpu_reference.rs:50-120).
+ *   - Batches are SoA / column-major: data[col * n + row] (src/lde/mod.rs:21).
+ *   - Results are bit-exact with the reference CPU path for every element.
+ *
+ * Threading: a context serialises its host-memory calls with an internal
+ * mutex; use one context per thread for concurrency.  Device-pointer (_dev)
+ * calls are asynchronous on the caller's stream; their device-resident tables
+ * must already be cached (sfntt_prepare) before a CUDA graph capture.
+ */
+#ifndef SFNTT_H
+#define SFNTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: one per NttError variant (src/ntt/mod.rs:52-69) plus three. */
+typedef enum sfntt_status {
+    SFNTT_OK = 0,
+    SFNTT_INVALID_SIZE = 1,      /* NttError::InvalidSize(usize)               */
+    SFNTT_DEVICE_NOT_FOUND = 2,  /* NttError::DeviceNotFound                   */
+    SFNTT_ALLOC_FAILED = 3,      /* NttError::BufferAllocFailed{requested_bytes} */
+    SFNTT_KERNEL_LOAD = 4,       /* NttError::ShaderCompileError: no sm_100a image for this GPU */
+    SFNTT_GPU_EXECUTION = 5,     /* NttError::GpuExecutionError(String)        */
+    SFNTT_MISMATCH = 6,          /* NttError::CorrectnessMismatch{..}          */
+    SFNTT_UNSUPPORTED = 7,       /* V1 inverse: the reference panics (todo!()) */
+    SFNTT_TIMEOUT = 8,           /* a bounded device-side wait ran out         */
+    SFNTT_INVALID_ARGUMENT = 9   /* null pointer, bad enum, cold cache during capture */
+} sfntt_status;
+
+typedef enum sfntt_field {
+    SFNTT_M31 = 0,       /* Circle NTT (DCCT) over M31       */
+    SFNTT_BABYBEAR = 1   /* radix-2 NTT over BabyBear        */
+} sfntt_field;
+
+/* Algorithm variants of the reference shootout (src/ntt/mod.rs:17-25). */
+typedef enum sfntt_variant {
+    SFNTT_BEST = 0,
+    SFNTT_V1_CT_DIT_R2 = 1,    /* one kernel per layer (metal_ct_dit_r2.rs)            */
+    SFNTT_V2_CT_GS_R2 = 2,     /* per-layer large strides + one smem tile (metal_r2.rs) */
+    SFNTT_V3_STOCKHAM_R2 = 3,  /* out-of-place ping-pong (metal_stockham_r2.rs)        */
+    SFNTT_V4_CT_GS_R4 = 4      /* fused multi-layer smem passes (metal_ct_gs_r4.rs)     */
+} sfntt_variant;
+
+/* Coset-LDE forms (src/lde/mod.rs:43-107). */
+typedef enum sfntt_lde_mode {
+    SFNTT_LDE_FUSED = 0,   /* normalize+shift+zero-pad folded into the adjacent NTT passes */
+    SFNTT_LDE_UNFUSED = 1  /* iDFT -> normalize -> zero-pad -> shift -> DFT, one kernel each */
+} sfntt_lde_mode;
+
+typedef struct sfntt_ctx sfntt_ctx;
+
+/* ---- context: replaces MetalContext::new / backend ::new(shader_dir)
+ *      (src/gpu.rs:26-64, src/ntt/babybear/metal_ct_gs_r4.rs:44-85). */
+int sfntt_ctx_create(int device, sfntt_ctx **out);
+void sfntt_ctx_destroy(sfntt_ctx *ctx);
+const char *sfntt_status_string(int status);
+const char *sfntt_last_error(const sfntt_ctx *ctx);
+/* MetalContext::device_info (src/gpu.rs:132-150): "name, SMs, memory". */
+int sfntt_device_info(sfntt_ctx *ctx, char *buf, size_t len);
+
+/* ---- NttBackend<F>::forward_ntt / inverse_ntt (src/ntt/mod.rs:37-44):
+ * in place on host memory of len elements (power of two; len == 1 is the
+ * identity).  *gpu_ns (optional) receives the device time of the transform. */
+int sfntt_forward(sfntt_ctx *ctx, int field, int variant, uint32_t *data, size_t len,
+                  uint64_t *gpu_ns);
+int sfntt_inverse(sfntt_ctx *ctx, int field, int variant, uint32_t *data, size_t len,
+                  uint64_t *gpu_ns);
+
+/* ---- NttBackend<F>::pointwise_mul (src/ntt/mod.rs:46-48). */
+int sfntt_pointwise_mul(sfntt_ctx *ctx, int field, const uint32_t *a, size_t len_a,
+                        const uint32_t *b, size_t len_b, uint32_t *out, size_t len_out);
+
+/* ---- forward_ntt_gpu / inverse_ntt_gpu(input, log_n) -> (Vec<u32>, ns)
+ * (src/ntt/babybear/metal_ct_gs_r4.rs:87-172, src/ntt/m31/metal_ct_gs_r4.rs:61-99):
+ * out-of-place; len must equal 2^log_n. */
+int sfntt_forward_gpu(sfntt_ctx *ctx, int field, int variant, const uint32_t *in, size_t len,
+                      uint32_t log_n, uint32_t *out, uint64_t *gpu_ns);
+int sfntt_inverse_gpu(sfntt_ctx *ctx, int field, int variant, const uint32_t *in, size_t len,
+                      uint32_t log_n, uint32_t *out, uint64_t *gpu_ns);
+
+/* ---- BbBatchNtt::forward_ntt_batch_gpu / inverse_ntt_batch_gpu
+ * (src/ntt/babybear/batch.rs:76-180): batch SoA columns of 2^log_n; len must
+ * equal batch << log_n.  field = SFNTT_M31 batches the Circle NTT the same way. */
+int sfntt_forward_batch(sfntt_ctx *ctx, int field, const uint32_t *in, size_t len,
+                        uint32_t log_n, uint32_t batch, uint32_t *out, uint64_t *gpu_ns);
+int sfntt_inverse_batch(sfntt_ctx *ctx, int field, const uint32_t *in, size_t len,
+                        uint32_t log_n, uint32_t batch, uint32_t *out, uint64_t *gpu_ns);
+
+/* ---- CosetLdeBatch::execute(input, log_n, batch_size, added_bits)
+ * (src/lde/mod.rs:43-107).  in: batch columns of 2^log_n Montgomery u32
+ * (len must equal batch << log_n); out: batch columns of 2^(log_n+added_bits),
+ * bit-reversed rows.  shift_monty == 0 selects the reference shift
+ * two_adic_generator(log_n + added_bits + 1) (src/lde/mod.rs:59); any other
+ * value is a Montgomery-form shift (e.g. to_monty(31), the Plonky3 coset).
+ * Host buffers; copies are pipelined by column chunks with the compute. */
+int sfntt_bb_coset_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n,
+                       uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode,
+                       uint32_t *out, uint64_t *gpu_ns);
+
+/* M31 blow-up (no reference counterpart: the composition of the reference's
+ * inverse on odds(log_n), zero-pad, forward on odds(log_n + added_bits)). */
+int sfntt_m31_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n,
+                  uint32_t batch, uint32_t added_bits, uint32_t *out, uint64_t *gpu_ns);
+
+/* ---- device-pointer twins (stream = cudaStream_t; NULL = legacy default).
+ * Asynchronous; no host synchronisation and no allocation when the tables
+ * for (field, log_n) are cached. */
+int sfntt_prepare(sfntt_ctx *ctx, int field, uint32_t log_n);
+int sfntt_prepare_lde(sfntt_ctx *ctx, int field, uint32_t log_n, uint32_t added_bits,
+                      uint32_t shift_monty);
+int sfntt_forward_dev(sfntt_ctx *ctx, int field, int variant, uint32_t *d_data, uint32_t log_n,
+                      uint32_t batch, void *stream);
+int sfntt_inverse_dev(sfntt_ctx *ctx, int field, int variant, uint32_t *d_data, uint32_t log_n,
+                      uint32_t batch, void *stream);
+/* d_in is read only; d_out holds batch << (log_n + added_bits) elements. */
+int sfntt_bb_coset_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
+                           uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode,
+                           void *stream);
+int sfntt_m31_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
+                      uint32_t batch, uint32_t added_bits, void *stream);
+
+/* BabyBear::to_monty / from_monty (src/field/babybear.rs:54-65) on device. */
+int sfntt_bb_to_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
+int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
+
+/* Pinned host memory for the host-buffer calls (full-bandwidth copies). */
+int sfntt_host_alloc(sfntt_ctx *ctx, size_t bytes, void **out);
+int sfntt_host_free(sfntt_ctx *ctx, void *p);
+
+/* Number of kernels this library has launched through ctx (for launch counts). */
+uint64_t sfntt_launch_count(const sfntt_ctx *ctx);
+
+/* Tracing (the reference only times commit->wait, src/gpu.rs:229-232):
+ * sfntt_kernel_timing(ctx, 1) brackets every later launch with CUDA events
+ * (and clears earlier records); sfntt_kernel_times synchronises and writes one
+ * line per kernel: "<name> <launches> <total_ms> <algorithmic_bytes>\n". */
+int sfntt_kernel_timing(sfntt_ctx *ctx, int enable);
+int sfntt_kernel_times(sfntt_ctx *ctx, char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFNTT_H */

@@ -1,0 +1,174 @@
+// context.hpp -- internal state behind an sfntt_ctx: device, stream, the
+// device-resident twiddle / multiplier caches and the staging buffers used by
+// the host-memory entry points.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/sfntt.h"
+
+namespace sfntt {
+
+// Error carried from a failing step to the C ABI.
+struct Status {
+  int code = SFNTT_OK;
+  std::string msg;
+  bool ok() const { return code == SFNTT_OK; }
+};
+
+inline int map_cuda_error(cudaError_t e) {
+  switch (e) {
+    case cudaSuccess: return SFNTT_OK;
+    case cudaErrorMemoryAllocation: return SFNTT_ALLOC_FAILED;
+    case cudaErrorNoDevice:
+    case cudaErrorInvalidDevice:
+    case cudaErrorInsufficientDriver: return SFNTT_DEVICE_NOT_FOUND;
+    case cudaErrorNoKernelImageForDevice:
+    case cudaErrorInvalidDeviceFunction:
+    case cudaErrorInvalidKernelImage: return SFNTT_KERNEL_LOAD;
+    default: return SFNTT_GPU_EXECUTION;
+  }
+}
+
+#define SFNTT_CU(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return ::sfntt::Status{::sfntt::map_cuda_error(e_),                              \
+                             std::string(#call) + ": " + cudaGetErrorString(e_)};      \
+  } while (0)
+
+#define SFNTT_TRY(expr)                  \
+  do {                                   \
+    ::sfntt::Status s_ = (expr);         \
+    if (!s_.ok()) return s_;             \
+  } while (0)
+
+// Device buffer owned by a context (grow-only).
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  Status reserve(size_t want) {
+    if (want <= bytes) return {};
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return {SFNTT_ALLOC_FAILED, "cudaMalloc(" + std::to_string(want) + " bytes) failed"};
+    }
+    bytes = want;
+    return {};
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace sfntt
+
+struct sfntt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;         // host-memory calls run here
+  cudaStream_t copy_streams[2] = {};     // H2D / D2H lanes of the pipelined LDE
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  std::recursive_mutex mu;
+  std::string last_error;
+  int sm_count = 0;
+  std::atomic<uint64_t> launches{0};
+
+  // Twiddle tables: BabyBear per-layer Shoup pairs (layer s at 2^s - 1),
+  // shared by every n <= 2^bb_log[dir]; M31 per log_n (layer l at n - n/2^l).
+  sfntt::DevBuf bb_tw[2];
+  uint32_t bb_log[2] = {0, 0};
+  std::map<uint32_t, sfntt::DevBuf> m31_tw[2];
+  // LDE multiplier tables keyed by (log_n, added_bits, shift, kind)
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, sfntt::DevBuf> lde_tabs;
+
+  // staging for host-memory calls
+  sfntt::DevBuf buf_in, buf_out, buf_aux;
+
+  // Opt-in per-kernel timing (sfntt_kernel_timing): an event pair around every
+  // launch, resolved and aggregated by name in sfntt_kernel_times.
+  struct TimedLaunch { std::string name; uint64_t bytes; cudaEvent_t start, stop; };
+  bool timing = false;
+  std::vector<TimedLaunch> timed;
+  cudaEvent_t pending_start = nullptr;
+};
+
+namespace sfntt {
+
+// Table accessors (twiddles.cu).  All generate on a miss (allocating) and
+// refuse to do so while `stream` is capturing.
+Status bb_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
+Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
+// kind 0: fused LDE multipliers M_q[i] = n^-1 (shift g^{rev(q)})^i, q < 2^added, i < n
+// kind 1: plain shift powers shift^i, i < n_ext (unfused path)
+Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty, int kind,
+                    cudaStream_t stream, const uint2** out);
+
+// Kernel drivers (ntt.cu / lde.cu / elementwise.cu)
+Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d_data, uint32_t log_n,
+               uint32_t batch, cudaStream_t stream);
+Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in, uint32_t* d_out,
+                   uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize,
+                   cudaStream_t stream);
+Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
+Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                   uint32_t added_bits, cudaStream_t stream);
+Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                         size_t n, cudaStream_t stream);
+Status bb_monty_dev(sfntt_ctx* ctx, bool to_monty, uint32_t* d, size_t n, cudaStream_t stream);
+Status scale_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint64_t n, uint32_t w_canonical, cudaStream_t stream);
+Status zero_pad_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t log_n, uint32_t batch,
+                    uint32_t added_bits, cudaStream_t stream);
+Status mul_table_dev(sfntt_ctx* ctx, uint32_t* d, uint32_t log_n_ext, uint32_t batch, const uint2* tab,
+                     cudaStream_t stream);
+
+inline void count_launch(sfntt_ctx* ctx, uint64_t n = 1) { ctx->launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Call right before a kernel launch on stream s (records the start event when
+// per-kernel timing is on).
+inline void launch_begin(sfntt_ctx* ctx, cudaStream_t s) {
+  if (!ctx->timing) return;
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) == cudaSuccess && cudaEventRecord(e, s) == cudaSuccess) ctx->pending_start = e;
+}
+
+// Call right after the launch: checks the launch, counts it and, when timing
+// is on, closes the event pair under `what` with its algorithmic HBM bytes.
+inline Status launch_check(sfntt_ctx* ctx, const char* what, cudaStream_t s = nullptr, uint64_t bytes = 0) {
+  count_launch(ctx);
+  cudaError_t e = cudaGetLastError();
+  if (ctx->timing && ctx->pending_start) {
+    cudaEvent_t stop = nullptr;
+    if (cudaEventCreate(&stop) == cudaSuccess && cudaEventRecord(stop, s) == cudaSuccess)
+      ctx->timed.push_back({what, bytes, ctx->pending_start, stop});
+    ctx->pending_start = nullptr;
+  }
+  if (e != cudaSuccess) return {map_cuda_error(e), std::string(what) + ": " + cudaGetErrorString(e)};
+  return {};
+}
+
+inline bool capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return st != cudaStreamCaptureStatusNone;
+}
+
+}  // namespace sfntt

@@ -1,0 +1,261 @@
+// lde.cu -- batched coset low-degree extension (src/lde/mod.rs:43-107).
+//
+// Reference pipeline per column: iDFT (size n) -> x n^-1 -> zero-pad to
+// n_ext = n 2^b -> x shift^i -> forward DFT (size n_ext), output bit-reversed.
+//
+// Fused form (three kernels for n > 2^12, one below):
+//   I1  inverse layers [0, lo) of every column, input -> output buffer
+//   X   one tile kernel per group of 2^P points: inverse layers [lo, log_n),
+//       then for each of the 2^b output blocks q: multiply by
+//         M_q[i] = n^-1 * shift^i * g_ext^(i * rev_b(q)),
+//       which is the normalisation, the coset shift and the top b layers of the
+//       zero-padded DIF (whose upper inputs are zero, so each of those layers
+//       reduces to "copy, and copy times twiddle"), then forward layers
+//       [lo, log_n) of block q, stored to output rows [q n, (q+1) n)
+//   F3  forward layers [0, lo) of the n_ext-point network, in place
+// Every HBM byte of the input is read once and every output byte is written
+// twice (X and F3), against the reference's separate iDFT / normalize+pad+
+// shift / DFT passes.
+//
+// Unfused form ("plain"): iDFT -> normalize -> zero-pad -> coset shift -> DFT,
+// one kernel (family) each, as in the reference's never-dispatched
+// bb_zero_pad_batch / bb_coset_shift_batch (shaders/babybear/bb_ntt_r2.metal:379-415).
+//
+// M31 blow-up: iDFT (normalised) -> replicate into the 2^b blocks (the CT
+// butterflies of the top b layers see a zero upper half, so they only copy)
+// -> forward layers [0, log_n) of the n_ext network.
+#include <algorithm>
+#include <string>
+
+#include "context.hpp"
+#include "field.cuh"
+#include "host_field.hpp"
+#include "ntt_launch.cuh"
+
+namespace sfntt {
+
+Status ntt_layers_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint64_t stride, uint32_t log_n,
+                      uint32_t batch, uint32_t a, uint32_t b, cudaStream_t s);
+
+namespace {
+
+struct ExpandArgs {
+  PassArgs inv;        // geometry + inverse twiddles (in: source, out: destination)
+  const uint2* tw_fwd;
+  const uint2* mul;    // M_q table, q * n + i
+  uint32_t log_q;      // added bits
+};
+
+template <Kind KD, int P, int LT>
+struct Expand {
+  static constexpr int CB = P + LT;
+  static constexpr int R = CB < 4 ? CB : 4;
+  using Inv = Pass<BabyBear, false, KD, P, LT, R>;
+  using Fwd = Pass<BabyBear, true, KD, P, LT, R>;
+  static constexpr int K = Inv::K;
+  static constexpr int E = Inv::E;
+  static constexpr int NT = Inv::NT;
+  static constexpr int SMEM_WORDS = Inv::SMEM_WORDS;
+
+  __device__ static __forceinline__ uint32_t pos_of(const TileGeo& g, uint32_t c, const PassArgs& a) {
+    if constexpr (KD == Kind::S) return g.pos_base | Inv::map_pos(c, a.lo);
+    else return g.spans ? ((g.v0 + c) & ((1u << a.log_n) - 1u)) : (g.pos_base + c);
+  }
+
+  __device__ static __forceinline__ uint32_t* out_ptr(const TileGeo& g, uint32_t c, const PassArgs& a) {
+    if constexpr (KD == Kind::C) {
+      if (g.spans) return a.out + (uint64_t)((g.v0 + c) >> a.log_n) * a.out_stride;
+    }
+    return g.out;
+  }
+
+  __device__ static void run(const ExpandArgs& ea) {
+    extern __shared__ uint32_t sm[];
+    const uint32_t tid = threadIdx.x;
+    const PassArgs& ai = ea.inv;
+    PassArgs af = ea.inv;
+    af.tw = ea.tw_fwd;
+    const TileGeo g = Inv::geometry(ai);
+    uint32_t x[E];
+    Inv::template load_global<0>(x, g, ai, tid);
+    Inv::template rounds_from<0>(sm, x, g, ai, tid);  // ends in round K-1's layout, values in [0, 2p)
+
+    using M = RM<KD, P, LT, R, K - 1>;
+    using M0 = RM<KD, P, LT, R, 0>;
+    const uint32_t ct = M::ctid(tid);
+    const uint32_t ct0 = M0::ctid(tid);
+    const uint32_t n = 1u << ai.log_n;
+    const uint32_t nq = 1u << ea.log_q;
+    for (uint32_t q = 0; q < nq; ++q) {
+      uint32_t v[E];
+      const uint2* mq = ea.mul + (uint64_t)q * n;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const uint2 w = __ldg(&mq[pos_of(g, ct | M::cm(m), ai)]);
+        v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
+      }
+      __syncthreads();  // the previous block's last shared-memory reads are done
+      Fwd::template rounds_from<0>(sm, v, g, af, tid);  // forward starts in round K-1's layout
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const uint32_t c = ct0 | M0::cm(m);
+        out_ptr(g, c, ai)[(uint64_t)q * n + pos_of(g, c, ai)] = v[m];
+      }
+    }
+  }
+};
+
+template <Kind KD, int P, int LT>
+__global__ void __launch_bounds__(Expand<KD, P, LT>::NT) expand_kernel(ExpandArgs ea) {
+  Expand<KD, P, LT>::run(ea);
+}
+
+template <Kind KD, int P, int LT>
+constexpr int CB_of() { return P + LT; }
+
+template <Kind KD, int P, int LT>
+Status launch_expand(sfntt_ctx* ctx, const ExpandArgs& ea, uint32_t tiles, cudaStream_t s) {
+  using X = Expand<KD, P, LT>;
+  constexpr int smem = X::SMEM_WORDS * 4;
+  auto kern = expand_kernel<KD, P, LT>;
+  if (smem > 48 * 1024) SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  launch_begin(ctx, s);
+  kern<<<tiles, X::NT, smem, s>>>(ea);
+  // reads 2^CB points per tile, writes 2^(CB + added_bits)
+  const uint64_t bytes = ((uint64_t)tiles << (CB_of<KD, P, LT>() + 2)) * (1u + (1u << ea.log_q));
+  static const std::string name = std::string("bb_lde_expand_") + (KD == Kind::C ? "C" : "S") + std::to_string(P);
+  return launch_check(ctx, name.c_str(), s, bytes);
+}
+
+// Expand tiles: 2^13 points for both kinds (strided: 8 low positions).
+__host__ __device__ constexpr int x_lt_s(int P) { return P <= 10 ? 3 : 13 - P; }
+
+#define SFNTT_X_CASE(PP)                                                                       \
+  case PP:                                                                                     \
+    if (contiguous) {                                                                          \
+      if (full) return launch_expand<Kind::C, PP, kCTileBits - PP>(ctx, ea, tiles_full, s);   \
+      return launch_expand<Kind::C, PP, 0>(ctx, ea, tiles_single, s);                         \
+    }                                                                                          \
+    return launch_expand<Kind::S, PP, x_lt_s(PP)>(ctx, ea, tiles_s, s);
+
+Status run_expand(sfntt_ctx* ctx, ExpandArgs ea, int P, uint32_t batch, cudaStream_t s) {
+  const bool contiguous = ea.inv.lo == 0;
+  const uint32_t log_n = ea.inv.log_n;
+  ea.inv.batch = batch;
+  const bool full = (int)log_n + ctz32(batch) >= kCTileBits;
+  const uint64_t total = (uint64_t)batch << log_n;
+  const uint32_t tiles_full = (uint32_t)(total >> kCTileBits);
+  const uint32_t tiles_single = (uint32_t)(total >> P);
+  uint32_t tiles_s = 0;
+  if (!contiguous) {
+    const int lt = x_lt_s(P);
+    if ((int)ea.inv.lo < lt || ea.inv.lo + P != log_n) return {SFNTT_INVALID_ARGUMENT, "expand geometry"};
+    ea.inv.log_tiles_per_col = log_n - P - lt;
+    tiles_s = batch << ea.inv.log_tiles_per_col;
+  }
+  switch (P) {
+    SFNTT_X_CASE(1) SFNTT_X_CASE(2) SFNTT_X_CASE(3) SFNTT_X_CASE(4) SFNTT_X_CASE(5) SFNTT_X_CASE(6)
+    SFNTT_X_CASE(7) SFNTT_X_CASE(8) SFNTT_X_CASE(9) SFNTT_X_CASE(10) SFNTT_X_CASE(11) SFNTT_X_CASE(12)
+    default: break;
+  }
+  return {SFNTT_INVALID_ARGUMENT, "unsupported expand size"};
+}
+#undef SFNTT_X_CASE
+
+// out[c n_ext + q n + r] = out[c n_ext + r] for q in [1, 2^b)
+__global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, uint64_t total) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = i >> log_n;
+    const uint32_t r = (uint32_t)(i & ((1ull << log_n) - 1ull));
+    const uint32_t v = d[(c << log_ext) + r];
+    for (uint32_t q = 1; q < (1u << (log_ext - log_n)); ++q) d[(c << log_ext) + ((uint64_t)q << log_n) + r] = v;
+  }
+}
+
+}  // namespace
+
+Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+  if (mode != SFNTT_LDE_FUSED && mode != SFNTT_LDE_UNFUSED) return {SFNTT_INVALID_ARGUMENT, "unknown LDE mode"};
+  const uint32_t log_ext = log_n + added_bits;
+  if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
+  if (batch == 0) return {};
+  const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
+  const bool fused = mode == SFNTT_LDE_FUSED && log_n >= 1 && log_n <= 24 && added_bits <= 4;
+  if (fused) {
+    const uint2 *tw_inv = nullptr, *tw_fwd = nullptr, *mul = nullptr;
+    SFNTT_TRY(bb_twiddles(ctx, true, log_n, s, &tw_inv));
+    SFNTT_TRY(bb_twiddles(ctx, false, log_ext, s, &tw_fwd));
+    SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 0, s, &mul));
+    const uint32_t lo = log_n <= 12 ? 0u : (log_n + 1) / 2;
+    const int P = (int)(log_n - lo);
+    if (lo > 0) {  // I1: inverse layers [0, lo) into the output buffer
+      PassRequest r{};
+      r.args.in = d_in; r.args.out = d_out; r.args.tw = tw_inv;
+      r.args.in_stride = n; r.args.out_stride = n_ext;
+      r.args.log_n = log_n; r.args.lo = 0; r.P = (int)lo; r.contiguous = true; r.batch = batch;
+      SFNTT_TRY(run_pass_bb_inv(ctx, r, s));
+    }
+    ExpandArgs ea{};
+    ea.inv.in = lo > 0 ? d_out : d_in;
+    ea.inv.out = d_out;
+    ea.inv.tw = tw_inv;
+    ea.inv.in_stride = lo > 0 ? n_ext : n;
+    ea.inv.out_stride = n_ext;
+    ea.inv.log_n = log_n;
+    ea.inv.lo = lo;
+    ea.tw_fwd = tw_fwd;
+    ea.mul = mul;
+    ea.log_q = added_bits;
+    SFNTT_TRY(run_expand(ctx, ea, P, batch, s));
+    if (lo > 0) {  // F3: forward layers [0, lo) of the n_ext network
+      PassRequest r{};
+      r.args.in = d_out; r.args.out = d_out; r.args.tw = tw_fwd;
+      r.args.in_stride = n_ext; r.args.out_stride = n_ext;
+      r.args.log_n = log_ext; r.args.lo = 0; r.P = (int)lo; r.contiguous = true; r.batch = batch;
+      SFNTT_TRY(run_pass_bb_fwd(ctx, r, s));
+    }
+    return {};
+  }
+  // unfused: iDFT (no normalize) into scratch, normalize, zero-pad, shift, DFT
+  const size_t bytes = (size_t)(n * batch) * sizeof(uint32_t);
+  if (capturing(s) && ctx->buf_aux.bytes < bytes) return {SFNTT_INVALID_ARGUMENT, "LDE scratch not prepared"};
+  SFNTT_TRY(ctx->buf_aux.reserve(bytes));
+  uint32_t* coeffs = ctx->buf_aux.as<uint32_t>();
+  if (log_n > 0) {
+    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_BABYBEAR, true, d_in, coeffs, n, n, log_n, batch, false, s));
+    SFNTT_TRY(scale_dev(ctx, SFNTT_BABYBEAR, coeffs, n * batch, host::invmod((uint32_t)n, host::BB_P), s));
+  } else {
+    SFNTT_CU(cudaMemcpyAsync(coeffs, d_in, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  SFNTT_TRY(zero_pad_dev(ctx, coeffs, d_out, log_n, batch, added_bits, s));
+  const uint2* shift_tab = nullptr;
+  SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 1, s, &shift_tab));
+  SFNTT_TRY(mul_table_dev(ctx, d_out, log_ext, batch, shift_tab, s));
+  if (log_ext > 0) SFNTT_TRY(ntt_dev(ctx, SFNTT_BABYBEAR, SFNTT_V4_CT_GS_R4, false, d_out, log_ext, batch, s));
+  return {};
+}
+
+Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                   uint32_t added_bits, cudaStream_t s) {
+  const uint32_t log_ext = log_n + added_bits;
+  if (log_ext > 30) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
+  if (batch == 0) return {};
+  const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
+  if (log_n > 0) {
+    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, true, s));
+  } else {
+    SFNTT_CU(cudaMemcpy2DAsync(d_out, n_ext * 4, d_in, 4, 4, batch, cudaMemcpyDeviceToDevice, s));
+  }
+  if (added_bits > 0) {
+    const uint64_t total = (uint64_t)batch << log_n;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)ctx->sm_count * 16);
+    launch_begin(ctx, s);
+    replicate_kernel<<<grid ? grid : 1, 256, 0, s>>>(d_out, log_n, log_ext, total);
+    SFNTT_TRY(launch_check(ctx, "m31_replicate", s, total * 4u * (1u + (1u << added_bits) - 1u)));
+  }
+  if (log_n > 0) SFNTT_TRY(ntt_layers_dev(ctx, SFNTT_M31, false, d_out, n_ext, log_ext, batch, 0, log_n, s));
+  return {};
+}
+
+}  // namespace sfntt

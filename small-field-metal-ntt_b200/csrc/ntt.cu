@@ -1,0 +1,291 @@
+// ntt.cu -- transform planning (which layers go to which pass), the V1-V3
+// algorithm variants of the reference shootout, and the small elementwise
+// kernels (normalize, zero-pad, coset shift, pointwise product, Montgomery
+// conversion).
+#include <algorithm>
+
+#include "context.hpp"
+#include "field.cuh"
+#include "host_field.hpp"
+#include "ntt_launch.cuh"
+
+namespace sfntt {
+
+static Status run_pass(sfntt_ctx* ctx, int field, bool desc, const PassRequest& r, cudaStream_t s) {
+  if (field == SFNTT_BABYBEAR) return desc ? run_pass_bb_fwd(ctx, r, s) : run_pass_bb_inv(ctx, r, s);
+  return desc ? run_pass_m31_fwd(ctx, r, s) : run_pass_m31_inv(ctx, r, s);
+}
+
+// Split layers [a, b) into passes of at most 12 layers, as even as possible,
+// the lowest pass taking the remainder.  Returns the number of passes.
+static int split_layers(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
+  const uint32_t total = b - a;
+  const int k = (int)((total + 11) / 12);
+  for (int i = 0; i < k; ++i) cnt[i] = total / k + ((uint32_t)i < total % k ? 1u : 0u);
+  uint32_t s = a;
+  for (int i = 0; i < k; ++i) { lo[i] = s; s += cnt[i]; }
+  return k;
+}
+
+static Status get_tw(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, cudaStream_t s, const uint2** tw) {
+  if (field == SFNTT_BABYBEAR) return bb_twiddles(ctx, inverse, log_n, s, tw);
+  return m31_twiddles(ctx, inverse, log_n, s, tw);
+}
+
+static uint32_t inv_n_canonical(int field, uint32_t log_n) {
+  const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
+  return host::invmod(host::powmod(2, log_n, p), p);
+}
+
+// Runs layers [a, b) of the 2^log_n-point network (forward: descending, CT/GS
+// per field; inverse: ascending) on `batch` columns.  The first pass reads
+// `in`, later passes work in place on `out`.  scale_w != 0 multiplies every
+// output of the last pass by the canonical constant scale_w.
+static Status run_layers(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out,
+                         uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a,
+                         uint32_t b, uint32_t scale_w, const uint2* tw, cudaStream_t s) {
+  uint32_t lo[4], cnt[4];
+  const int k = split_layers(a, b, lo, cnt);
+  const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
+  for (int i = 0; i < k; ++i) {
+    const int pi = inverse ? i : (k - 1 - i);  // forward runs the high layers first
+    PassRequest r{};
+    r.args.in = (i == 0) ? in : out;
+    r.args.out = out;
+    r.args.tw = tw;
+    r.args.in_stride = (i == 0) ? in_stride : out_stride;
+    r.args.out_stride = out_stride;
+    r.args.log_n = log_n;
+    r.args.lo = lo[pi];
+    r.args.scale = (i == k - 1 && scale_w) ? 1 : 0;
+    r.args.scale_w = scale_w;
+    r.args.scale_ws = host::shoup(scale_w, p);
+    r.P = (int)cnt[pi];
+    r.contiguous = (lo[pi] == 0);
+    r.batch = batch;
+    SFNTT_TRY(run_pass(ctx, field, !inverse, r, s));
+  }
+  return {};
+}
+
+// ---------------------------------------------------------------- V1 / V3 ---
+// One radix-2 layer over all columns: the per-layer dispatch of the
+// reference's V1 (src/ntt/*/metal_ct_dit_r2.rs) and, out of place, V3
+// (src/ntt/*/metal_stockham_r2.rs).  Same butterflies, same twiddles.
+template <class F, bool DESC>
+__global__ void layer_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint2* __restrict__ tw,
+                             uint32_t log_n, uint32_t L, uint64_t pairs, uint32_t scale, uint32_t sw, uint32_t sws) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= pairs) return;
+  const uint32_t half_pairs_log = log_n - 1;
+  const uint64_t col = t >> half_pairs_log;
+  const uint32_t k = (uint32_t)(t & ((1ull << half_pairs_log) - 1ull));
+  const uint32_t j = k & ((1u << L) - 1u);
+  const uint32_t blk = k >> L;
+  const uint32_t i0 = (blk << (L + 1)) + j;
+  const uint32_t i1 = i0 + (1u << L);
+  const uint64_t base = col << log_n;
+  uint32_t a = in[base + i0], b = in[base + i1];
+  uint2 w;
+  if constexpr (F::kMontgomery) w = tw[((1u << L) - 1u) + j];
+  else w = tw[((1u << log_n) - (1u << (log_n - L))) + blk];
+  if constexpr (F::kMontgomery == DESC) {  // GS
+    const uint32_t s = add_mod<F>(a, b);
+    b = mul_shoup<F>(a - b + F::P, w.x, w.y);
+    a = s;
+  } else {  // CT, canonical in and out
+    const uint32_t x = mul_shoup<F>(b, w.x, w.y);
+    b = sub_mod<F>(a, x);
+    a = add_mod<F>(a, x);
+  }
+  if (scale) {
+    a = mul_shoup<F>(a, sw, sws);
+    b = mul_shoup<F>(b, sw, sws);
+  }
+  out[base + i0] = a;
+  out[base + i1] = b;
+}
+
+template <class F, bool DESC>
+static Status launch_layer(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, const uint2* tw, uint32_t log_n,
+                           uint32_t L, uint32_t batch, uint32_t scale_w, cudaStream_t s) {
+  const uint64_t pairs = (uint64_t)batch << (log_n - 1);
+  const uint32_t blocks = (uint32_t)((pairs + 255) / 256);
+  launch_begin(ctx, s);
+  layer_kernel<F, DESC><<<blocks, 256, 0, s>>>(in, out, tw, log_n, L, pairs, scale_w ? 1u : 0u, scale_w,
+                                                 host::shoup(scale_w, F::P));
+  return launch_check(ctx, F::kMontgomery ? "bb_layer" : "m31_layer", s, pairs * 16u);
+}
+
+static Status layer(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, const uint2* tw,
+                    uint32_t log_n, uint32_t L, uint32_t batch, uint32_t scale_w, cudaStream_t s) {
+  if (field == SFNTT_BABYBEAR)
+    return inverse ? launch_layer<BabyBear, false>(ctx, in, out, tw, log_n, L, batch, scale_w, s)
+                   : launch_layer<BabyBear, true>(ctx, in, out, tw, log_n, L, batch, scale_w, s);
+  return inverse ? launch_layer<M31, false>(ctx, in, out, tw, log_n, L, batch, scale_w, s)
+                 : launch_layer<M31, true>(ctx, in, out, tw, log_n, L, batch, scale_w, s);
+}
+
+// ----------------------------------------------------------------- driver ---
+Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d, uint32_t log_n, uint32_t batch,
+               cudaStream_t s) {
+  if (field != SFNTT_BABYBEAR && field != SFNTT_M31) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
+  if (variant < SFNTT_BEST || variant > SFNTT_V4_CT_GS_R4) return {SFNTT_INVALID_ARGUMENT, "unknown variant"};
+  if (field == SFNTT_BABYBEAR && log_n > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n > 27"};
+  if (field == SFNTT_M31 && log_n > 30) return {SFNTT_INVALID_SIZE, "log_n > 30"};
+  if (log_n >= 32 || ((uint64_t)batch << log_n) >= (1ull << 40)) return {SFNTT_INVALID_SIZE, "too large"};
+  if (variant == SFNTT_V1_CT_DIT_R2 && inverse)
+    return {SFNTT_UNSUPPORTED, "V1 (CT-DIT r2) has no inverse, as in the reference (todo!())"};
+  if (log_n == 0 || batch == 0) return {};
+  const uint2* tw = nullptr;
+  SFNTT_TRY(get_tw(ctx, field, inverse, log_n, s, &tw));
+  const uint32_t scale = inverse ? inv_n_canonical(field, log_n) : 0u;
+  const uint64_t stride = 1ull << log_n;
+  switch (variant) {
+    case SFNTT_V1_CT_DIT_R2: {
+      for (int L = (int)log_n - 1; L >= 0; --L)
+        SFNTT_TRY(layer(ctx, field, false, d, d, tw, log_n, (uint32_t)L, batch, 0, s));
+      return {};
+    }
+    case SFNTT_V2_CT_GS_R2: {
+      // large strides one layer per kernel, then the low layers in one tile pass
+      const uint32_t tile = std::min<uint32_t>(log_n, 12);
+      if (!inverse) {
+        for (int L = (int)log_n - 1; L >= (int)tile; --L)
+          SFNTT_TRY(layer(ctx, field, false, d, d, tw, log_n, (uint32_t)L, batch, 0, s));
+        return run_layers(ctx, field, false, d, d, stride, stride, log_n, batch, 0, tile, 0, tw, s);
+      }
+      SFNTT_TRY(run_layers(ctx, field, true, d, d, stride, stride, log_n, batch, 0, tile,
+                           tile == log_n ? scale : 0u, tw, s));
+      for (uint32_t L = tile; L < log_n; ++L)
+        SFNTT_TRY(layer(ctx, field, true, d, d, tw, log_n, L, batch, L + 1 == log_n ? scale : 0u, s));
+      return {};
+    }
+    case SFNTT_V3_STOCKHAM_R2: {
+      // out-of-place ping-pong between the caller's buffer and a scratch buffer
+      const size_t bytes = ((size_t)batch << log_n) * sizeof(uint32_t);
+      if (capturing(s) && ctx->buf_aux.bytes < bytes)
+        return {SFNTT_INVALID_ARGUMENT, "V3 scratch not prepared before capture"};
+      SFNTT_TRY(ctx->buf_aux.reserve(bytes));
+      uint32_t* bufs[2] = {d, ctx->buf_aux.as<uint32_t>()};
+      int cur = 0;
+      for (uint32_t i = 0; i < log_n; ++i) {
+        const uint32_t L = inverse ? i : log_n - 1 - i;
+        SFNTT_TRY(layer(ctx, field, inverse, bufs[cur], bufs[cur ^ 1], tw, log_n, L, batch,
+                        (inverse && i + 1 == log_n) ? scale : 0u, s));
+        cur ^= 1;
+      }
+      if (cur != 0) SFNTT_CU(cudaMemcpyAsync(d, bufs[1], bytes, cudaMemcpyDeviceToDevice, s));
+      return {};
+    }
+    default:
+      return run_layers(ctx, field, inverse, d, d, stride, stride, log_n, batch, 0, log_n, scale, tw, s);
+  }
+}
+
+Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
+                   uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize, cudaStream_t s) {
+  if (log_n == 0 || batch == 0) return {SFNTT_INVALID_ARGUMENT, "empty transform"};
+  const uint2* tw = nullptr;
+  SFNTT_TRY(get_tw(ctx, field, inverse, log_n, s, &tw));
+  const uint32_t scale = (inverse && normalize) ? inv_n_canonical(field, log_n) : 0u;
+  return run_layers(ctx, field, inverse, in, out, in_stride, out_stride, log_n, batch, 0, log_n, scale, tw, s);
+}
+
+// Layers [a, b) of a forward / inverse network, in place; used by the M31
+// blow-up whose zero-padded top layers are a plain replication.
+Status ntt_layers_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint64_t stride, uint32_t log_n,
+                      uint32_t batch, uint32_t a, uint32_t b, cudaStream_t s) {
+  const uint2* tw = nullptr;
+  SFNTT_TRY(get_tw(ctx, field, inverse, log_n, s, &tw));
+  return run_layers(ctx, field, inverse, d, d, stride, stride, log_n, batch, a, b, 0u, tw, s);
+}
+
+// ------------------------------------------------------------ elementwise ---
+namespace {
+
+template <class F>
+__global__ void scale_kernel(uint32_t* d, uint64_t n, uint32_t w, uint32_t ws) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    d[i] = mul_shoup<F>(d[i], w, ws);
+}
+
+template <class F>
+__global__ void pointwise_kernel(const uint32_t* a, const uint32_t* b, uint32_t* out, uint64_t n) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = mul_var<F>(a[i], b[i]);
+}
+
+__global__ void monty_kernel(uint32_t* d, uint64_t n, int to) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    d[i] = to ? mul_var<BabyBear>(d[i], BabyBear::R2) : mul_var<BabyBear>(d[i], 1u);
+}
+
+// out[c * n_ext + r] = r < n ? in[c * n + r] : 0   (bb_zero_pad_batch, shaders/babybear/bb_ntt_r2.metal:379-398)
+__global__ void zero_pad_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t log_n,
+                                uint32_t log_ext, uint64_t total) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t c = i >> log_ext;
+    const uint32_t r = (uint32_t)(i & ((1ull << log_ext) - 1ull));
+    out[i] = (r < (1u << log_n)) ? in[(c << log_n) + r] : 0u;
+  }
+}
+
+// d[c * n_ext + i] *= tab[i]   (bb_coset_shift_batch, shaders/babybear/bb_ntt_r2.metal:402-415)
+__global__ void mul_table_kernel(uint32_t* d, uint32_t log_ext, uint64_t total, const uint2* __restrict__ tab) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 w = tab[i & ((1ull << log_ext) - 1ull)];
+    d[i] = mul_shoup<BabyBear>(d[i], w.x, w.y);
+  }
+}
+
+uint32_t grid_for(sfntt_ctx* ctx, uint64_t n) {
+  const uint64_t want = (n + 255) / 256;
+  const uint64_t cap = (uint64_t)ctx->sm_count * 16;
+  return (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
+}
+
+}  // namespace
+
+Status scale_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint64_t n, uint32_t w, cudaStream_t s) {
+  launch_begin(ctx, s);
+  if (field == SFNTT_BABYBEAR)
+    scale_kernel<BabyBear><<<grid_for(ctx, n), 256, 0, s>>>(d, n, w, host::shoup(w, host::BB_P));
+  else
+    scale_kernel<M31><<<grid_for(ctx, n), 256, 0, s>>>(d, n, w, host::shoup(w, host::M31_P));
+  return launch_check(ctx, "scale", s, n * 8u);
+}
+
+Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uint32_t* b, uint32_t* out, size_t n,
+                         cudaStream_t s) {
+  if (n == 0) return {};
+  launch_begin(ctx, s);
+  if (field == SFNTT_BABYBEAR) pointwise_kernel<BabyBear><<<grid_for(ctx, n), 256, 0, s>>>(a, b, out, n);
+  else pointwise_kernel<M31><<<grid_for(ctx, n), 256, 0, s>>>(a, b, out, n);
+  return launch_check(ctx, "pointwise_mul", s, (uint64_t)n * 12u);
+}
+
+Status bb_monty_dev(sfntt_ctx* ctx, bool to, uint32_t* d, size_t n, cudaStream_t s) {
+  if (n == 0) return {};
+  launch_begin(ctx, s);
+  monty_kernel<<<grid_for(ctx, n), 256, 0, s>>>(d, n, to ? 1 : 0);
+  return launch_check(ctx, to ? "bb_to_monty" : "bb_from_monty", s, (uint64_t)n * 8u);
+}
+
+Status zero_pad_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t log_n, uint32_t batch,
+                    uint32_t added_bits, cudaStream_t s) {
+  const uint64_t total = (uint64_t)batch << (log_n + added_bits);
+  launch_begin(ctx, s);
+  zero_pad_kernel<<<grid_for(ctx, total), 256, 0, s>>>(in, out, log_n, log_n + added_bits, total);
+  return launch_check(ctx, "bb_zero_pad", s, total * 4u + ((uint64_t)batch << log_n) * 4u);
+}
+
+Status mul_table_dev(sfntt_ctx* ctx, uint32_t* d, uint32_t log_ext, uint32_t batch, const uint2* tab,
+                     cudaStream_t s) {
+  const uint64_t total = (uint64_t)batch << log_ext;
+  launch_begin(ctx, s);
+  mul_table_kernel<<<grid_for(ctx, total), 256, 0, s>>>(d, log_ext, total, tab);
+  return launch_check(ctx, "bb_coset_shift", s, total * 8u);
+}
+
+}  // namespace sfntt

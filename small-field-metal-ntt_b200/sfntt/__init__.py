@@ -1,0 +1,398 @@
+"""sfntt -- Python mirror of the reference's NTT / coset-LDE API over libsfntt.so.
+
+The reference (moven0831/small-field-metal-ntt) exposes, in Rust:
+  * trait NttBackend<F> { name, forward_ntt, inverse_ntt, pointwise_mul }
+    (src/ntt/mod.rs:26-49) and the NttError enum (src/ntt/mod.rs:52-69);
+  * per-variant backends V1..V4 for M31 and BabyBear with inherent
+    forward_ntt_gpu / inverse_ntt_gpu (e.g. src/ntt/babybear/metal_ct_gs_r4.rs:87-172);
+  * BbBatchNtt::forward_ntt_batch_gpu / inverse_ntt_batch_gpu
+    (src/ntt/babybear/batch.rs:76-180);
+  * CosetLdeBatch::new / execute -> LdeResult { data, total_ns } (src/lde/mod.rs:15-107).
+This module provides the same names, argument meanings and error behaviour on
+top of the CUDA library.  Field elements are numpy uint32 arrays holding the
+reference's raw representation (M31 canonical, BabyBear Montgomery form).
+The reference type names (MetalCtGsR4, BbMetalCtGsR4, ...) are kept as aliases
+so that code written against the reference switches by import only.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _ffi
+
+M31_P = 2147483647
+BB_P = 2013265921
+FIELD_M31 = 0
+FIELD_BABYBEAR = 1
+BEST, V1, V2, V3, V4 = 0, 1, 2, 3, 4
+LDE_FUSED, LDE_UNFUSED = 0, 1
+
+
+# --------------------------------------------------------------- errors ---
+class NttError(Exception):
+    """NttError (src/ntt/mod.rs:52-69)."""
+    status = -1
+
+
+class InvalidSize(NttError):
+    status = 1
+
+    def __init__(self, size: int, detail: str = ""):
+        self.size = size
+        super().__init__(f"Invalid NTT size: {size} (must be power of 2){': ' + detail if detail else ''}")
+
+
+class DeviceNotFound(NttError):
+    status = 2
+
+
+class BufferAllocFailed(NttError):
+    status = 3
+
+    def __init__(self, msg: str = "", requested_bytes: int | None = None):
+        self.requested_bytes = requested_bytes
+        super().__init__(msg)
+
+
+class ShaderCompileError(NttError):
+    """No loadable sm_100a kernel image for this device (the reference's
+    runtime shader-compilation failure)."""
+    status = 4
+
+
+class GpuExecutionError(NttError):
+    status = 5
+
+
+class CorrectnessMismatch(NttError):
+    status = 6
+
+    def __init__(self, index: int, expected: int, got: int):
+        self.index, self.expected, self.got = index, expected, got
+        super().__init__(f"Correctness mismatch at index {index}: expected {expected}, got {got}")
+
+
+class Unsupported(NttError):
+    """The reference panics here (V1 inverse is todo!())."""
+    status = 7
+
+
+class Timeout(NttError):
+    status = 8
+
+
+class InvalidArgument(NttError):
+    status = 9
+
+
+_ERRORS = {1: InvalidSize, 2: DeviceNotFound, 3: BufferAllocFailed, 4: ShaderCompileError,
+           5: GpuExecutionError, 7: Unsupported, 8: Timeout, 9: InvalidArgument}
+
+
+def _check(ctx, status: int, size: int = 0) -> None:
+    if status == 0:
+        return
+    L = _ffi.lib()
+    detail = L.sfntt_last_error(ctx).decode() if ctx else ""
+    cls = _ERRORS.get(status, NttError)
+    if cls is InvalidSize:
+        raise InvalidSize(size, detail)
+    raise cls(f"{L.sfntt_status_string(status).decode()}: {detail}")
+
+
+# -------------------------------------------------------------- context ---
+class Context:
+    """A device context (the reference's MetalContext, src/gpu.rs:26-64):
+    stream, device-resident twiddle caches and staging buffers."""
+
+    def __init__(self, device: int = 0):
+        L = _ffi.lib()
+        h = ctypes.c_void_p()
+        st = L.sfntt_ctx_create(device, ctypes.byref(h))
+        if st != 0:
+            cls = _ERRORS.get(st, NttError)
+            raise cls(f"sfntt_ctx_create(device={device}): {L.sfntt_status_string(st).decode()}")
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            _ffi.lib().sfntt_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_info(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        _check(self.handle, _ffi.lib().sfntt_device_info(self.handle, buf, 256))
+        return buf.value.decode()
+
+    def launch_count(self) -> int:
+        return int(_ffi.lib().sfntt_launch_count(self.handle))
+
+    def kernel_timing(self, enable: bool = True) -> None:
+        """Bracket every later launch with CUDA events (clears old records)."""
+        _check(self.handle, _ffi.lib().sfntt_kernel_timing(self.handle, int(enable)))
+
+    def kernel_times(self) -> dict:
+        """{kernel: (launches, total_ms, algorithmic_bytes)} since kernel_timing()."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        _check(self.handle, _ffi.lib().sfntt_kernel_times(self.handle, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, launches, ms, nbytes = line.split()
+            out[name] = (int(launches), float(ms), int(nbytes))
+        return out
+
+    def prepare(self, field: int, log_n: int) -> None:
+        _check(self.handle, _ffi.lib().sfntt_prepare(self.handle, field, log_n))
+
+    def prepare_lde(self, field: int, log_n: int, added_bits: int, shift_monty: int = 0) -> None:
+        _check(self.handle, _ffi.lib().sfntt_prepare_lde(self.handle, field, log_n, added_bits, shift_monty))
+
+    def pinned(self, n: int) -> "PinnedBuffer":
+        """Page-locked host buffer of n uint32 (full-bandwidth copies)."""
+        return PinnedBuffer(self, n)
+
+
+class PinnedBuffer:
+    """Pinned host memory from sfntt_host_alloc; `.array` is a numpy view."""
+
+    def __init__(self, ctx: Context, n: int):
+        self.ctx = ctx
+        p = ctypes.c_void_p()
+        _check(ctx.handle, _ffi.lib().sfntt_host_alloc(ctx.handle, max(n, 1) * 4, ctypes.byref(p)))
+        self.addr = p.value
+        self.array = np.ctypeslib.as_array((ctypes.c_uint32 * max(n, 1)).from_address(self.addr))[:n]
+
+    def free(self) -> None:
+        if self.addr and self.ctx.handle:
+            self.array = None
+            _ffi.lib().sfntt_host_free(self.ctx.handle, ctypes.c_void_p(self.addr))
+        self.addr = 0
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+_DEFAULT: dict[int, Context] = {}
+
+
+def default_context(device: int = 0) -> Context:
+    if device not in _DEFAULT:
+        _DEFAULT[device] = Context(device)
+    return _DEFAULT[device]
+
+
+def _u32(a) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+    return arr
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_ffi.u32p) if a.size else None
+
+
+# ------------------------------------------------------------- backends ---
+class NttBackend:
+    """trait NttBackend<F> (src/ntt/mod.rs:26-49), in place on uint32 arrays."""
+
+    FIELD = FIELD_BABYBEAR
+    VARIANT = BEST
+    NAME = "cuda"
+
+    def __init__(self, ctx: Context | None = None, device: int = 0):
+        self.ctx = ctx or default_context(device)
+
+    @classmethod
+    def new(cls, shader_dir=None, device: int = 0):
+        """Same shape as the reference's `new(shader_dir)`; the directory is
+        not needed (kernels are compiled ahead of time for sm_100a)."""
+        return cls(device=device)
+
+    def name(self) -> str:
+        return self.NAME
+
+    def _inplace(self, fn, data) -> None:
+        arr = data if isinstance(data, np.ndarray) and data.dtype == np.uint32 and data.flags["C_CONTIGUOUS"] \
+            else None
+        work = arr if arr is not None else _u32(data).copy()
+        ns = ctypes.c_uint64()
+        st = fn(self.ctx.handle, self.FIELD, self.VARIANT, _p(work), work.size, ctypes.byref(ns))
+        _check(self.ctx.handle, st, work.size)
+        if arr is None:
+            data[:] = [int(v) for v in work]
+
+    def forward_ntt(self, data, twiddles: Sequence[int] = ()) -> None:
+        """Coefficients -> evaluations (bit-reversed order), in place.
+        `twiddles` is ignored, as by every reference backend (src/ntt/mod.rs:33-36)."""
+        self._inplace(_ffi.lib().sfntt_forward, data)
+
+    def inverse_ntt(self, data, twiddles: Sequence[int] = ()) -> None:
+        """Bit-reversed evaluations -> coefficients (x n^-1), in place."""
+        self._inplace(_ffi.lib().sfntt_inverse, data)
+
+    def pointwise_mul(self, a, b, out) -> None:
+        a_, b_ = _u32(a), _u32(b)
+        o = out if isinstance(out, np.ndarray) and out.dtype == np.uint32 and out.flags["C_CONTIGUOUS"] else None
+        work = o if o is not None else np.empty(len(out), dtype=np.uint32)
+        st = _ffi.lib().sfntt_pointwise_mul(self.ctx.handle, self.FIELD, _p(a_), a_.size, _p(b_), b_.size,
+                                            _p(work), work.size)
+        _check(self.ctx.handle, st, a_.size)
+        if o is None:
+            out[:] = [int(v) for v in work]
+
+    def _gpu(self, fn, input, log_n: int):
+        inp = _u32(input)
+        out = np.empty_like(inp)
+        ns = ctypes.c_uint64()
+        st = fn(self.ctx.handle, self.FIELD, self.VARIANT, _p(inp), inp.size, log_n, _p(out), ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return out, int(ns.value)
+
+    def forward_ntt_gpu(self, input, log_n: int):
+        """-> (output, device ns) (src/ntt/babybear/metal_ct_gs_r4.rs:87-120)."""
+        return self._gpu(_ffi.lib().sfntt_forward_gpu, input, log_n)
+
+    def inverse_ntt_gpu(self, input, log_n: int):
+        return self._gpu(_ffi.lib().sfntt_inverse_gpu, input, log_n)
+
+    # batched SoA columns (BbBatchNtt, src/ntt/babybear/batch.rs:76-180)
+    def _batch(self, fn, input, log_n: int, batch: int):
+        inp = _u32(input)
+        out = np.empty_like(inp)
+        ns = ctypes.c_uint64()
+        st = fn(self.ctx.handle, self.FIELD, _p(inp), inp.size, log_n, batch, _p(out), ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return out, int(ns.value)
+
+    def forward_ntt_batch_gpu(self, input, log_n: int, batch: int):
+        return self._batch(_ffi.lib().sfntt_forward_batch, input, log_n, batch)
+
+    def inverse_ntt_batch_gpu(self, input, log_n: int, batch: int):
+        return self._batch(_ffi.lib().sfntt_inverse_batch, input, log_n, batch)
+
+    # device pointers (e.g. torch tensors' data_ptr()) on a CUDA stream handle
+    def forward_dev(self, ptr: int, log_n: int, batch: int = 1, stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_forward_dev(self.ctx.handle, self.FIELD, self.VARIANT, ptr, log_n, batch, stream)
+        _check(self.ctx.handle, st, batch << log_n)
+
+    def inverse_dev(self, ptr: int, log_n: int, batch: int = 1, stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_inverse_dev(self.ctx.handle, self.FIELD, self.VARIANT, ptr, log_n, batch, stream)
+        _check(self.ctx.handle, st, batch << log_n)
+
+
+# M31 Circle NTT (DCCT) variants (src/ntt/m31/*)
+class CudaCtDitR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_M31, V1, "cuda-ct-dit-r2"
+
+
+class CudaCtGsR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_M31, V2, "cuda-ct-gs-r2"
+
+
+class CudaStockhamR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_M31, V3, "cuda-stockham-r2"
+
+
+class CudaCtGsR4(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_M31, V4, "cuda-ct-gs-r4"
+
+
+# BabyBear variants (src/ntt/babybear/*)
+class BbCudaCtDitR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_BABYBEAR, V1, "bb-cuda-ct-dit-r2"
+
+
+class BbBatchNtt(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_BABYBEAR, V2, "bb-cuda-r2"
+
+
+class BbCudaStockhamR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_BABYBEAR, V3, "bb-cuda-stockham-r2"
+
+
+class BbCudaCtGsR4(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_BABYBEAR, V4, "bb-cuda-ct-gs-r4"
+
+
+# reference type names (src/ntt/m31/*, src/ntt/babybear/*, src/ntt/metal_r2.rs:337-340)
+MetalCtDitR2, MetalCtGsR2, MetalStockhamR2, MetalCtGsR4 = CudaCtDitR2, CudaCtGsR2, CudaStockhamR2, CudaCtGsR4
+BbMetalCtDitR2, BbMetalR2, BbMetalStockhamR2, BbMetalCtGsR4 = BbCudaCtDitR2, BbBatchNtt, BbCudaStockhamR2, BbCudaCtGsR4
+
+
+# -------------------------------------------------------------------- LDE ---
+@dataclass
+class LdeResult:
+    """LdeResult (src/lde/mod.rs:20-25): SoA data[col * n_ext + row]."""
+    data: np.ndarray
+    total_ns: int
+
+
+class CosetLdeBatch:
+    """CosetLdeBatch (src/lde/mod.rs:15-107)."""
+
+    def __init__(self, ctx: Context | None = None, device: int = 0, fused: bool = True):
+        self.ctx = ctx or default_context(device)
+        self.mode = LDE_FUSED if fused else LDE_UNFUSED
+
+    @classmethod
+    def new(cls, shader_dir=None, device: int = 0):
+        return cls(device=device)
+
+    def execute(self, input, log_n: int, batch_size: int, added_bits: int, shift_monty: int = 0,
+                out: np.ndarray | None = None) -> LdeResult:
+        inp = _u32(input)
+        n_out = batch_size << (log_n + added_bits)
+        dst = out if out is not None else np.empty(n_out, dtype=np.uint32)
+        ns = ctypes.c_uint64()
+        st = _ffi.lib().sfntt_bb_coset_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits,
+                                           shift_monty, self.mode, _p(dst), ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return LdeResult(dst, int(ns.value))
+
+    def execute_dev(self, in_ptr: int, out_ptr: int, log_n: int, batch_size: int, added_bits: int,
+                    shift_monty: int = 0, stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_bb_coset_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits,
+                                               shift_monty, self.mode, stream)
+        _check(self.ctx.handle, st, batch_size << log_n)
+
+    def device_info(self) -> str:
+        return self.ctx.device_info()
+
+
+class M31Lde:
+    """M31 blow-up: inverse on odds(log n) -> zero-pad -> forward on
+    odds(log n + added_bits).  No reference counterpart (the reference has no
+    M31 LDE); defined as that composition of reference functions."""
+
+    def __init__(self, ctx: Context | None = None, device: int = 0):
+        self.ctx = ctx or default_context(device)
+
+    def execute(self, input, log_n: int, batch_size: int, added_bits: int) -> LdeResult:
+        inp = _u32(input)
+        dst = np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
+        ns = ctypes.c_uint64()
+        st = _ffi.lib().sfntt_m31_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits,
+                                      _p(dst), ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return LdeResult(dst, int(ns.value))
+
+    def execute_dev(self, in_ptr: int, out_ptr: int, log_n: int, batch_size: int, added_bits: int,
+                    stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_m31_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits, stream)
+        _check(self.ctx.handle, st, batch_size << log_n)
+
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,65 @@
+"""ctypes binding of lib/libsfntt.so (declared in include/sfntt.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+PKG_ROOT = Path(__file__).resolve().parents[1]
+LIB_PATH = Path(os.environ.get("SFNTT_LIB", PKG_ROOT / "lib" / "libsfntt.so"))
+
+u32, u64, sz, i32 = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t, ctypes.c_int
+vp = ctypes.c_void_p
+u32p = ctypes.POINTER(ctypes.c_uint32)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+
+# name -> (restype, argtypes); mirrors include/sfntt.h one to one
+SIGNATURES = {
+    "sfntt_ctx_create": (i32, [i32, ctypes.POINTER(vp)]),
+    "sfntt_ctx_destroy": (None, [vp]),
+    "sfntt_status_string": (ctypes.c_char_p, [i32]),
+    "sfntt_last_error": (ctypes.c_char_p, [vp]),
+    "sfntt_device_info": (i32, [vp, ctypes.c_char_p, sz]),
+    "sfntt_forward": (i32, [vp, i32, i32, u32p, sz, u64p]),
+    "sfntt_inverse": (i32, [vp, i32, i32, u32p, sz, u64p]),
+    "sfntt_pointwise_mul": (i32, [vp, i32, u32p, sz, u32p, sz, u32p, sz]),
+    "sfntt_forward_gpu": (i32, [vp, i32, i32, u32p, sz, u32, u32p, u64p]),
+    "sfntt_inverse_gpu": (i32, [vp, i32, i32, u32p, sz, u32, u32p, u64p]),
+    "sfntt_forward_batch": (i32, [vp, i32, u32p, sz, u32, u32, u32p, u64p]),
+    "sfntt_inverse_batch": (i32, [vp, i32, u32p, sz, u32, u32, u32p, u64p]),
+    "sfntt_bb_coset_lde": (i32, [vp, u32p, sz, u32, u32, u32, u32, i32, u32p, u64p]),
+    "sfntt_m31_lde": (i32, [vp, u32p, sz, u32, u32, u32, u32p, u64p]),
+    "sfntt_prepare": (i32, [vp, i32, u32]),
+    "sfntt_prepare_lde": (i32, [vp, i32, u32, u32, u32]),
+    "sfntt_forward_dev": (i32, [vp, i32, i32, vp, u32, u32, vp]),
+    "sfntt_inverse_dev": (i32, [vp, i32, i32, vp, u32, u32, vp]),
+    "sfntt_bb_coset_lde_dev": (i32, [vp, vp, vp, u32, u32, u32, u32, i32, vp]),
+    "sfntt_m31_lde_dev": (i32, [vp, vp, vp, u32, u32, u32, vp]),
+    "sfntt_bb_to_monty_dev": (i32, [vp, vp, sz, vp]),
+    "sfntt_bb_from_monty_dev": (i32, [vp, vp, sz, vp]),
+    "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
+    "sfntt_host_free": (i32, [vp, vp]),
+    "sfntt_launch_count": (u64, [vp]),
+    "sfntt_kernel_timing": (i32, [vp, i32]),
+    "sfntt_kernel_times": (i32, [vp, ctypes.c_char_p, sz]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise OSError(f"{LIB_PATH} is missing: build it with `make -C small-field-metal-ntt_b200` "
+                          "(there is no CPU fallback)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib

@@ -1,0 +1,268 @@
+"""GPU parity: every CUDA path against the C oracle, bit for bit.
+
+Mirrors the reference's GPU test strategy (src/ntt/test_utils.rs:61-168,
+tests/ntt_cross_validation.rs:186-486, src/lde/mod.rs:194-271): forward vs CPU,
+round trip, edge cases (zeros, size 1, invalid / empty sizes), pointwise
+product, batch == per-column, coset LDE vs coset_lde_batch_cpu.  All calls go
+through the C ABI (sfntt -> libsfntt.so).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import sfntt
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+BB, M31 = sfntt.FIELD_BABYBEAR, sfntt.FIELD_M31
+P = {BB: O.BB_P, M31: O.M31_P}
+M31_BACKENDS = [sfntt.CudaCtDitR2, sfntt.CudaCtGsR2, sfntt.CudaStockhamR2, sfntt.CudaCtGsR4]
+BB_BACKENDS = [sfntt.BbCudaCtDitR2, sfntt.BbBatchNtt, sfntt.BbCudaStockhamR2, sfntt.BbCudaCtGsR4]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return sfntt.default_context(0)
+
+
+def data(field, n, seed):
+    return O.lcg(n, seed, P[field], monty=(field == BB))
+
+
+def ofwd(field, x):
+    return O.bb_forward(x) if field == BB else O.m31_forward(x)
+
+
+def oinv(field, x):
+    return O.bb_inverse(x) if field == BB else O.m31_inverse(x)
+
+
+# ---- golden fixtures straight through the GPU --------------------------------
+def test_gpu_matches_golden_fixtures(ctx, golden):
+    meta, arr = golden
+    for key, cls, inverse in (("bb_forward", sfntt.BbCudaCtGsR4, False), ("bb_inverse", sfntt.BbCudaCtGsR4, True),
+                              ("m31_forward", sfntt.CudaCtGsR4, False), ("m31_inverse", sfntt.CudaCtGsR4, True)):
+        b = cls(ctx)
+        for case in meta[key]:
+            x = arr[case["input"]].copy()
+            (b.inverse_ntt if inverse else b.forward_ntt)(x)
+            assert np.array_equal(x, arr[case["output"]]), (key, case["log_n"])
+    lde = sfntt.CosetLdeBatch(ctx)
+    for case in meta["bb_lde"]:
+        if "input" not in case:
+            continue
+        r = lde.execute(arr[case["input"]], case["log_n"], case["batch"], case["added_bits"],
+                        case.get("shift_monty", 0))
+        assert np.array_equal(r.data, arr[case["output"]]), case
+
+
+# ---- single-column forward / inverse, every variant ------------------------
+@pytest.mark.parametrize("cls", M31_BACKENDS + BB_BACKENDS, ids=lambda c: c.NAME)
+def test_forward_matches_cpu_all_sizes(ctx, cls):
+    f = cls.FIELD
+    b = cls(ctx)
+    for log_n in range(1, 17):
+        x = data(f, 1 << log_n, (1 << log_n) * 11111 + 98765)
+        y = x.copy()
+        b.forward_ntt(y)
+        assert np.array_equal(y, ofwd(f, x)), (cls.NAME, log_n)
+
+
+@pytest.mark.parametrize("cls", [c for c in M31_BACKENDS + BB_BACKENDS if c.VARIANT != sfntt.V1],
+                         ids=lambda c: c.NAME)
+def test_inverse_matches_cpu_and_roundtrips(ctx, cls):
+    f = cls.FIELD
+    b = cls(ctx)
+    for log_n in range(1, 17):
+        x = data(f, 1 << log_n, 7 + log_n)
+        y = x.copy()
+        b.inverse_ntt(y)
+        assert np.array_equal(y, oinv(f, x)), (cls.NAME, log_n)
+        z = x.copy()
+        b.forward_ntt(z)
+        assert not np.array_equal(z, x)
+        b.inverse_ntt(z)
+        assert np.array_equal(z, x), (cls.NAME, log_n)
+
+
+@pytest.mark.parametrize("log_n", [17, 18, 20, 22, 24])
+def test_bb_large_sizes_match_cpu(ctx, log_n):
+    b = sfntt.BbCudaCtGsR4(ctx)
+    x = data(BB, 1 << log_n, 12345 + log_n)
+    fw, _ = b.forward_ntt_gpu(x, log_n)
+    assert np.array_equal(fw, O.bb_forward(x))
+    iv, _ = b.inverse_ntt_gpu(x, log_n)
+    assert np.array_equal(iv, O.bb_inverse(x))
+
+
+@pytest.mark.parametrize("log_n", [17, 18, 20])
+def test_m31_large_sizes_match_cpu(ctx, log_n):
+    b = sfntt.CudaCtGsR4(ctx)
+    x = data(M31, 1 << log_n, 999 + log_n)
+    fw, _ = b.forward_ntt_gpu(x, log_n)
+    assert np.array_equal(fw, O.m31_forward(x))
+    iv, _ = b.inverse_ntt_gpu(x, log_n)
+    assert np.array_equal(iv, O.m31_inverse(x))
+
+
+@pytest.mark.parametrize("field", [BB, M31])
+def test_roundtrip_up_to_2_24(ctx, field):
+    b = (sfntt.BbCudaCtGsR4 if field == BB else sfntt.CudaCtGsR4)(ctx)
+    for log_n in (21, 23, 24):
+        x = data(field, 1 << log_n, log_n)
+        fw, _ = b.forward_ntt_gpu(x, log_n)
+        back, _ = b.inverse_ntt_gpu(fw, log_n)
+        assert np.array_equal(back, x), log_n
+        assert np.all(fw < P[field])
+
+
+def test_bb_27_bit_transform_roundtrip(ctx):
+    # largest BabyBear size (two-adicity 27) goes through the three-pass plan
+    log_n = 25
+    b = sfntt.BbCudaCtGsR4(ctx)
+    x = data(BB, 1 << log_n, 3)
+    fw, _ = b.forward_ntt_gpu(x, log_n)
+    back, _ = b.inverse_ntt_gpu(fw, log_n)
+    assert np.array_equal(back, x)
+    # linearity against a second input at the same size
+    y = data(BB, 1 << log_n, 4)
+    fy, _ = b.forward_ntt_gpu(y, log_n)
+    s = ((x.astype(np.uint64) + y) % O.BB_P).astype(np.uint32)
+    fs, _ = b.forward_ntt_gpu(s, log_n)
+    assert np.array_equal(fs, ((fw.astype(np.uint64) + fy) % O.BB_P).astype(np.uint32))
+
+
+# ---- edge cases (src/ntt/test_utils.rs:104-153) ------------------------------
+@pytest.mark.parametrize("cls", M31_BACKENDS + BB_BACKENDS, ids=lambda c: c.NAME)
+def test_edge_cases(ctx, cls):
+    b = cls(ctx)
+    z = np.zeros(64, np.uint32)
+    b.forward_ntt(z)
+    assert not z.any()
+    one = np.array([O.bb_to_monty(42) if cls.FIELD == BB else 42], np.uint32)
+    before = one.copy()
+    b.forward_ntt(one)
+    assert np.array_equal(one, before)
+    for bad in (np.ones(3, np.uint32), np.zeros(0, np.uint32)):
+        with pytest.raises(sfntt.InvalidSize):
+            b.forward_ntt(bad)
+        with pytest.raises(sfntt.InvalidSize):
+            b.inverse_ntt(bad)
+    if cls.VARIANT == sfntt.V1:
+        with pytest.raises(sfntt.Unsupported):
+            b.inverse_ntt(np.ones(8, np.uint32))
+    else:
+        one = before.copy()
+        b.inverse_ntt(one)
+        assert np.array_equal(one, before)
+
+
+def test_m31_constant_poly_is_all_ones(ctx):  # ntt_cross_validation.rs:634-645
+    for cls in M31_BACKENDS:
+        x = np.zeros(16, np.uint32)
+        x[0] = 1
+        cls(ctx).forward_ntt(x)
+        assert np.all(x == 1), cls.NAME
+
+
+def test_m31_size_limit(ctx):
+    b = sfntt.CudaCtGsR4(ctx)
+    with pytest.raises(sfntt.InvalidSize):
+        b.forward_ntt_gpu(np.zeros(1, np.uint32), 31)
+
+
+def test_pointwise_mul(ctx):  # test_utils.rs:156-168
+    m = sfntt.CudaCtGsR4(ctx)
+    out = np.zeros(4, np.uint32)
+    m.pointwise_mul([2, 3, 4, 5], [10, 20, 30, 40], out)
+    assert list(out) == [20, 60, 120, 200]
+    with pytest.raises(sfntt.InvalidSize):
+        m.pointwise_mul(np.ones(4, np.uint32), np.ones(3, np.uint32), np.zeros(4, np.uint32))
+    bb = sfntt.BbCudaCtGsR4(ctx)
+    a, b = data(BB, 1000, 1), data(BB, 1000, 2)
+    out = np.zeros(1000, np.uint32)
+    bb.pointwise_mul(a, b, out)
+    assert list(out) == [O.bb_mul(int(x), int(y)) for x, y in zip(a, b)]
+
+
+def test_bb_polynomial_multiplication(ctx):  # ntt_cross_validation.rs:113-148
+    b = sfntt.BbCudaCtGsR4(ctx)
+    x = np.array([O.bb_to_monty(1), O.bb_to_monty(2), 0, 0], np.uint32)
+    y = np.array([O.bb_to_monty(3), O.bb_to_monty(4), 0, 0], np.uint32)
+    b.forward_ntt(x)
+    b.forward_ntt(y)
+    c = np.zeros(4, np.uint32)
+    b.pointwise_mul(x, y, c)
+    b.inverse_ntt(c)
+    assert [O.bb_from_monty(int(v)) for v in c] == [3, 10, 8, 0]
+
+
+# ---- batches (src/ntt/babybear/batch.rs:438-505) -------------------------------
+@pytest.mark.parametrize("field", [BB, M31])
+@pytest.mark.parametrize("log_n,batch", [(1, 5), (4, 3), (8, 64), (10, 7), (12, 2), (13, 1), (14, 16), (20, 3)])
+def test_batch_equals_single(ctx, field, log_n, batch):
+    b = (sfntt.BbBatchNtt if field == BB else sfntt.CudaCtGsR4)(ctx)
+    x = data(field, batch << log_n, 100 + log_n)
+    fw, _ = b.forward_ntt_batch_gpu(x, log_n, batch)
+    n = 1 << log_n
+    for c in range(batch):
+        assert np.array_equal(fw[c * n:(c + 1) * n], ofwd(field, x[c * n:(c + 1) * n])), c
+    back, _ = b.inverse_ntt_batch_gpu(fw, log_n, batch)
+    assert np.array_equal(back, x)
+    with pytest.raises(sfntt.InvalidSize):
+        b.forward_ntt_batch_gpu(x[:-1], log_n, batch)
+
+
+# ---- coset LDE (src/lde/mod.rs:194-271) ----------------------------------------
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("log_n,batch,added", [(8, 4, 1), (12, 8, 1), (8, 4, 2), (0, 3, 1), (1, 2, 2), (5, 3, 3),
+                                                (13, 2, 1), (14, 3, 2), (16, 4, 1), (18, 2, 1), (11, 5, 4),
+                                                (6, 2, 5)])
+def test_coset_lde_matches_cpu(ctx, fused, log_n, batch, added):
+    lde = sfntt.CosetLdeBatch(ctx, fused=fused)
+    x = O.lcg(batch << log_n, 42, O.BB_P, monty=True)
+    r = lde.execute(x, log_n, batch, added)
+    assert np.array_equal(r.data, O.bb_coset_lde(x, log_n, batch, added, threads=8))
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_coset_lde_plonky3_shift(ctx, fused):
+    sh = O.bb_to_monty(31)
+    x = O.lcg(4 << 14, 7, O.BB_P, monty=True)
+    r = sfntt.CosetLdeBatch(ctx, fused=fused).execute(x, 14, 4, 1, shift_monty=sh)
+    assert np.array_equal(r.data, O.bb_coset_lde(x, 14, 4, 1, sh, threads=4))
+
+
+def test_coset_lde_rejects_bad_length(ctx):
+    with pytest.raises(sfntt.InvalidSize):
+        sfntt.CosetLdeBatch(ctx).execute(np.zeros(100, np.uint32), 8, 4, 1)
+
+
+@pytest.mark.parametrize("added", [1, 2])
+def test_coset_lde_full_size_sampled_columns(ctx, added):
+    """2^20 x 256 (the headline shape): every column on the GPU, a sample of
+    columns against the oracle, and the low-degree property on all columns."""
+    log_n, batch = 20, 256 if added == 1 else 64
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    x = O.lcg(batch << log_n, 2024 + added, O.BB_P, monty=True)
+    r = sfntt.CosetLdeBatch(ctx).execute(x, log_n, batch, added)
+    for c in (0, 1, batch // 2, batch - 1):
+        assert np.array_equal(r.data[c * n_ext:(c + 1) * n_ext],
+                              O.bb_coset_lde(x[c * n:(c + 1) * n], log_n, 1, added)), c
+    # interpolating the extension gives a polynomial of degree < n on the coset
+    coeffs, _ = sfntt.BbBatchNtt(ctx).inverse_ntt_batch_gpu(r.data, log_n + added, batch)
+    coeffs = coeffs.reshape(batch, n_ext)
+    assert not coeffs[:, n:].any()
+
+
+def test_m31_lde_matches_composition(ctx, golden):
+    meta, arr = golden
+    m = sfntt.M31Lde(ctx)
+    for case in meta["m31_lde"]:
+        r = m.execute(arr[case["input"]], case["log_n"], case["batch"], case["added_bits"])
+        assert np.array_equal(r.data, arr[case["output"]])
+    for (ln, b, ab) in ((12, 3, 1), (14, 2, 2), (16, 2, 1)):
+        x = O.lcg(b << ln, ln, O.M31_P)
+        assert np.array_equal(m.execute(x, ln, b, ab).data, O.m31_lde(x, ln, b, ab, threads=4)), (ln, b, ab)
