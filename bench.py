@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true")
     return ap.parse_args()
 
 
@@ -59,7 +60,8 @@ def workload(a) -> dict:
             "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
             "shift": "two_adic_generator(log_n_ext+1) (reference default)",
             "layout": "SoA column-major, Montgomery u32",
-            "l2": "inputs larger than L2 (1 GiB in, 2 GiB out per step)"}
+            "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
+                  f"{4 * a.batch << (a.log_n + a.added_bits) >> 20} MiB out per step)"}
 
 
 def algorithmic_bytes(a) -> int:
@@ -298,7 +300,7 @@ def main() -> None:
         hin.free()
         hout.free()
 
-    secondary = secondary_metrics(ctx, sfntt, torch)
+    secondary = None if a.no_secondary else secondary_metrics(ctx, sfntt, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -145,6 +145,11 @@ int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *
 int sfntt_host_alloc(sfntt_ctx *ctx, size_t bytes, void **out);
 int sfntt_host_free(sfntt_ctx *ctx, void *p);
 
+/* Device-side waits (TMA tile arrival) are bounded; a kernel that gives up
+ * sets a flag in the context.  Host-memory calls check it and return
+ * SFNTT_TIMEOUT; after _dev calls, synchronise the stream and call this. */
+int sfntt_check_device_error(sfntt_ctx *ctx);
+
 /* Number of kernels this library has launched through ctx (for launch counts). */
 uint64_t sfntt_launch_count(const sfntt_ctx *ctx);
 

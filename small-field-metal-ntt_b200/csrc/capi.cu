@@ -3,6 +3,7 @@
 // column-chunk pipelined host-memory coset LDE.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -25,6 +26,17 @@ struct DeviceGuard {
     if (prev >= 0) cudaSetDevice(prev);
   }
 };
+
+// A kernel whose bounded wait ran out raised the context's device flag.
+Status device_flag(sfntt_ctx* ctx) {
+  int v = 0;
+  SFNTT_CU(cudaMemcpy(&v, ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v) {
+    cudaMemset(ctx->err.p, 0, sizeof(int));
+    return {SFNTT_TIMEOUT, "a device-side wait timed out (TMA tile never arrived)"};
+  }
+  return {};
+}
 
 int finish(sfntt_ctx* ctx, const Status& s) {
   if (ctx) ctx->last_error = s.ok() ? std::string() : s.msg;
@@ -66,6 +78,7 @@ Status run_host_ntt(sfntt_ctx* ctx, int field, int variant, bool inverse, const 
   SFNTT_CU(cudaEventRecord(ctx->ev_stop, ctx->stream));
   SFNTT_CU(cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   SFNTT_CU(cudaStreamSynchronize(ctx->stream));
+  SFNTT_TRY(device_flag(ctx));
   return elapsed_ns(ctx, ns);
 }
 
@@ -177,6 +190,7 @@ Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out
     cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
     st = {sfntt::map_cuda_error(e), std::string("LDE pipeline: ") + cudaGetErrorString(e)};
   }
+  if (st.ok()) st = device_flag(ctx);
   if (st.ok() && ns) {
     double total = 0;
     for (uint32_t c = 0; c < nchunks; ++c) {
@@ -228,7 +242,9 @@ int sfntt_ctx_create(int device, sfntt_ctx** out) {
   auto* ctx = new sfntt_ctx();
   ctx->device = device;
   ctx->sm_count = prop.multiProcessorCount;
-  bool ok = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) == cudaSuccess &&
+  if (const char* e = std::getenv("SFNTT_NO_TMA")) ctx->no_tma = e[0] == '1';
+  bool ok = ctx->err.reserve(sizeof(int)).ok() && cudaMemset(ctx->err.p, 0, sizeof(int)) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&ctx->copy_streams[0], cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&ctx->copy_streams[1], cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreate(&ctx->ev_start) == cudaSuccess && cudaEventCreate(&ctx->ev_stop) == cudaSuccess;
@@ -470,6 +486,13 @@ int sfntt_host_free(sfntt_ctx* ctx, void* p) {
 }
 
 uint64_t sfntt_launch_count(const sfntt_ctx* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+int sfntt_check_device_error(sfntt_ctx* ctx) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, device_flag(ctx));
+}
 
 int sfntt_kernel_timing(sfntt_ctx* ctx, int enable) {
   if (!ctx) return SFNTT_INVALID_ARGUMENT;

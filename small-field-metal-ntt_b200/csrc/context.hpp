@@ -98,6 +98,10 @@ struct sfntt_ctx {
 
   // staging for host-memory calls
   sfntt::DevBuf buf_in, buf_out, buf_aux;
+  // device int set by a kernel whose bounded wait ran out (SFNTT_TIMEOUT)
+  sfntt::DevBuf err;
+  // route every pass through the first (non-TMA) tile engine (tests / A-B)
+  bool no_tma = false;
 
   // Opt-in per-kernel timing (sfntt_kernel_timing): an event pair around every
   // launch, resolved and aggregated by name in sfntt_kernel_times.
@@ -121,6 +125,11 @@ Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_
 // Kernel drivers (ntt.cu / lde.cu / elementwise.cu)
 Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d_data, uint32_t log_n,
                uint32_t batch, cudaStream_t stream);
+// Layers [a, b) of a 2^log_n network on `batch` columns (first pass in -> out,
+// later passes in place); scale_w != 0 multiplies the final outputs.
+Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
+                  uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
+                  const uint2* tw, cudaStream_t stream);
 Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in, uint32_t* d_out,
                    uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize,
                    cudaStream_t stream);

@@ -31,6 +31,7 @@
 #include "field.cuh"
 #include "host_field.hpp"
 #include "ntt_launch.cuh"
+#include "tma_launch.cuh"
 
 namespace sfntt {
 
@@ -172,6 +173,36 @@ __global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, 
   }
 }
 
+template <int P>
+Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_stride, uint32_t* d_out, uint32_t log_n,
+                         uint32_t batch, uint32_t added_bits, const uint2* tw_inv, const uint2* tw_fwd,
+                         const uint2* mul, cudaStream_t s) {
+  using X = TExpand<P>;
+  const uint32_t lo = log_n - P;
+  const uint64_t n = 1ull << log_n, n_ext = n << added_bits;
+  CUtensorMap min, mout;
+  SFNTT_TRY(encode_s_map(&min, src, lo, P, 1, n, src_stride, batch));
+  SFNTT_TRY(encode_s_map(&mout, d_out, lo, P, 1ull << added_bits, n, n_ext, batch));
+  TmaArgs a{};
+  a.tw = tw_inv;
+  a.tw_fwd = tw_fwd;
+  a.mul = mul;
+  a.log_n = log_n;
+  a.lo = lo;
+  a.batch = batch;
+  a.log_q = added_bits;
+  a.err = ctx->err.as<int>();
+  a.ntiles = (uint32_t)(((uint64_t)batch * n) >> (P + 5));
+  constexpr int smem = 3 * (int)X::TBYTES + 16 + 1024;
+  auto kern = tma_expand_kernel<P>;
+  SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
+  launch_begin(ctx, s);
+  kern<<<grid, X::NT, smem, s>>>(min, mout, a);
+  static const std::string name = "bb_lde_expand_tma_S" + std::to_string(P);
+  return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
+}
+
 }  // namespace
 
 Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
@@ -187,6 +218,17 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
     SFNTT_TRY(bb_twiddles(ctx, true, log_n, s, &tw_inv));
     SFNTT_TRY(bb_twiddles(ctx, false, log_ext, s, &tw_fwd));
     SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 0, s, &mul));
+    const bool tma_ok = !ctx->no_tma && log_n >= 13 && aligned16(d_in) && aligned16(d_out);
+    if (tma_ok) {
+      // I1: inverse layers [0, log_n - 8) into the output buffer; X: the
+      // persistent TMA expand on 8-layer strided tiles; F3: forward [0, lo).
+      const uint32_t lo = log_n - 8;
+      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s));
+      SFNTT_TRY(launch_tma_expand<8>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s));
+      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd,
+                           s));
+      return {};
+    }
     const uint32_t lo = log_n <= 12 ? 0u : (log_n + 1) / 2;
     const int P = (int)(log_n - lo);
     if (lo > 0) {  // I1: inverse layers [0, lo) into the output buffer

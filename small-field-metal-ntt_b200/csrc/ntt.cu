@@ -8,8 +8,27 @@
 #include "field.cuh"
 #include "host_field.hpp"
 #include "ntt_launch.cuh"
+#include "tma_launch.cuh"
 
 namespace sfntt {
+
+static Status run_tma_pass(sfntt_ctx* ctx, int field, bool desc, const TmaRequest& r, cudaStream_t s) {
+  if (field == SFNTT_BABYBEAR) return desc ? run_tma_pass_bb_fwd(ctx, r, s) : run_tma_pass_bb_inv(ctx, r, s);
+  return desc ? run_tma_pass_m31_fwd(ctx, r, s) : run_tma_pass_m31_inv(ctx, r, s);
+}
+
+// TMA plan for layers [0, b): one contiguous pass of 5..12 layers, then
+// strided passes of 8 layers.
+static int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
+  if (a != 0) return 0;
+  const uint32_t s = b > 12 ? (b - 12 + 7) / 8 : 0;
+  const uint32_t c = b - 8 * s;
+  if (c < 5 || c > 12 || s > 3) return 0;
+  lo[0] = 0;
+  cnt[0] = c;
+  for (uint32_t i = 1; i <= s; ++i) { lo[i] = c + 8 * (i - 1); cnt[i] = 8; }
+  return (int)(1 + s);
+}
 
 static Status run_pass(sfntt_ctx* ctx, int field, bool desc, const PassRequest& r, cudaStream_t s) {
   if (field == SFNTT_BABYBEAR) return desc ? run_pass_bb_fwd(ctx, r, s) : run_pass_bb_inv(ctx, r, s);
@@ -41,10 +60,35 @@ static uint32_t inv_n_canonical(int field, uint32_t log_n) {
 // per field; inverse: ascending) on `batch` columns.  The first pass reads
 // `in`, later passes work in place on `out`.  scale_w != 0 multiplies every
 // output of the last pass by the canonical constant scale_w.
-static Status run_layers(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out,
-                         uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a,
-                         uint32_t b, uint32_t scale_w, const uint2* tw, cudaStream_t s) {
+Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
+                  uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
+                  const uint2* tw, cudaStream_t s) {
   uint32_t lo[4], cnt[4];
+  if (!ctx->no_tma) {
+    const int kt = tma_split(a, b, lo, cnt);
+    TmaRequest req[4];
+    bool ok = kt > 0;
+    for (int i = 0; i < kt && ok; ++i) {
+      const int pi = inverse ? i : (kt - 1 - i);
+      TmaRequest& r = req[i];
+      r.in = (i == 0) ? in : out;
+      r.out = out;
+      r.in_stride = (i == 0) ? in_stride : out_stride;
+      r.out_stride = out_stride;
+      r.tw = tw;
+      r.log_n = log_n;
+      r.lo = lo[pi];
+      r.P = (int)cnt[pi];
+      r.contiguous = lo[pi] == 0;
+      r.batch = batch;
+      r.scale_w = (i == kt - 1) ? scale_w : 0u;
+      ok = tma_pass_ok(r, field == SFNTT_M31);
+    }
+    if (ok) {
+      for (int i = 0; i < kt; ++i) SFNTT_TRY(run_tma_pass(ctx, field, !inverse, req[i], s));
+      return {};
+    }
+  }
   const int k = split_layers(a, b, lo, cnt);
   const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
   for (int i = 0; i < k; ++i) {
@@ -153,9 +197,9 @@ Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d
       if (!inverse) {
         for (int L = (int)log_n - 1; L >= (int)tile; --L)
           SFNTT_TRY(layer(ctx, field, false, d, d, tw, log_n, (uint32_t)L, batch, 0, s));
-        return run_layers(ctx, field, false, d, d, stride, stride, log_n, batch, 0, tile, 0, tw, s);
+        return layers_dev(ctx, field, false, d, d, stride, stride, log_n, batch, 0, tile, 0, tw, s);
       }
-      SFNTT_TRY(run_layers(ctx, field, true, d, d, stride, stride, log_n, batch, 0, tile,
+      SFNTT_TRY(layers_dev(ctx, field, true, d, d, stride, stride, log_n, batch, 0, tile,
                            tile == log_n ? scale : 0u, tw, s));
       for (uint32_t L = tile; L < log_n; ++L)
         SFNTT_TRY(layer(ctx, field, true, d, d, tw, log_n, L, batch, L + 1 == log_n ? scale : 0u, s));
@@ -179,7 +223,7 @@ Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d
       return {};
     }
     default:
-      return run_layers(ctx, field, inverse, d, d, stride, stride, log_n, batch, 0, log_n, scale, tw, s);
+      return layers_dev(ctx, field, inverse, d, d, stride, stride, log_n, batch, 0, log_n, scale, tw, s);
   }
 }
 
@@ -189,7 +233,7 @@ Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, 
   const uint2* tw = nullptr;
   SFNTT_TRY(get_tw(ctx, field, inverse, log_n, s, &tw));
   const uint32_t scale = (inverse && normalize) ? inv_n_canonical(field, log_n) : 0u;
-  return run_layers(ctx, field, inverse, in, out, in_stride, out_stride, log_n, batch, 0, log_n, scale, tw, s);
+  return layers_dev(ctx, field, inverse, in, out, in_stride, out_stride, log_n, batch, 0, log_n, scale, tw, s);
 }
 
 // Layers [a, b) of a forward / inverse network, in place; used by the M31
@@ -198,7 +242,7 @@ Status ntt_layers_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint
                       uint32_t batch, uint32_t a, uint32_t b, cudaStream_t s) {
   const uint2* tw = nullptr;
   SFNTT_TRY(get_tw(ctx, field, inverse, log_n, s, &tw));
-  return run_layers(ctx, field, inverse, d, d, stride, stride, log_n, batch, a, b, 0u, tw, s);
+  return layers_dev(ctx, field, inverse, d, d, stride, stride, log_n, batch, a, b, 0u, tw, s);
 }
 
 // ------------------------------------------------------------ elementwise ---

@@ -1,0 +1,373 @@
+// tile_tma.cuh -- persistent, TMA-fed version of the tile engine.
+//
+// Every tile is 2^13 words = 32 KiB = 256 rows of 128 bytes:
+//   Kind::C  2^13 consecutive words (2^(13-P) whole groups of 2^P points);
+//   Kind::S  32 consecutive low positions (one 128-byte row each) of a
+//            2^P-point group with stride 2^lo, P <= 8 (one TMA box {32,1,2^P}).
+// Each CTA owns a strided sequence of tiles.  Thread 0 keeps one tile in
+// flight ahead of the compute (double-buffered TMA loads into shared memory,
+// completion tracked by mbarriers) and writes finished tiles back with TMA
+// stores, so HBM traffic overlaps the integer work and moves with one
+// instruction per tile.  The rounds and butterflies are those of ntt_pass.cuh;
+// shared-memory exchanges happen in place in the staging buffer, with
+// compile-time address offsets and 128-bit accesses wherever a thread owns four
+// consecutive words.
+//
+// Every wait on an mbarrier is bounded (kWaitNs); a CTA that gives up sets the
+// error flag, waits for its own TMA stores and returns.
+#pragma once
+#include <cstdint>
+
+#include "ntt_pass.cuh"
+#include "tma.cuh"
+
+namespace sfntt {
+
+constexpr int kTileBits = 13;
+constexpr uint32_t kTileWords = 1u << kTileBits;
+constexpr uint32_t kTileBytes = 4u << kTileBits;
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: far beyond any tile's latency
+
+struct TmaArgs {
+  const uint2* tw;     // twiddles (layer-concatenated Shoup pairs)
+  uint32_t log_n;      // positions per column of this network
+  uint32_t lo;         // first global layer of the pass
+  uint32_t ntiles;
+  uint32_t log_tpc;    // Kind::C: log2(tiles per column) (n >= 2^13)
+  uint32_t batch;
+  uint32_t spans;      // Kind::C: tiles span columns (n < 2^13, dense columns)
+  uint32_t scale, scale_w, scale_ws;
+  int* err;
+  // fused LDE expansion (Expand kernel only)
+  const uint2* tw_fwd;
+  const uint2* mul;
+  uint32_t log_q;
+};
+
+// Where a tile sits: tensor-map coordinates and the column position of its
+// first word (shared by every pass type so fused kernels can mix directions).
+struct TileCoord {
+  uint32_t pos_base;  // Kind::C: column position of word 0; Kind::S: lchunk << 5
+  uint32_t hb;        // Kind::S high block
+  int32_t c1, c2;     // Kind::C map coordinates (row, column)
+  int32_t s1, s3, s4; // Kind::S map coordinates (lchunk, hb, column)
+};
+
+template <class F, bool DESC, Kind KD, int P>
+struct TPass {
+  static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
+  static constexpr int CB = P + LT;
+  static constexpr int R = 4;
+  static constexpr int NT = 1 << (CB - R);
+  static constexpr int E = 1 << R;
+  static constexpr int K = Plan<P, R>::K;
+  static_assert(KD == Kind::C ? CB == kTileBits : (P <= 8), "tile shape");
+  static constexpr uint32_t TWORDS = 1u << CB;
+  static constexpr uint32_t TBYTES = 4u << CB;
+
+  using Geo = TileCoord;
+
+  __device__ static __forceinline__ Geo geo(const TmaArgs& a, uint32_t t) {
+    Geo g{};
+    if constexpr (KD == Kind::C) {
+      if (a.spans) {
+        g.pos_base = 0;
+        g.c1 = (int32_t)(t << (CB - 5));
+        g.c2 = 0;
+      } else {
+        const uint32_t r = t & ((1u << a.log_tpc) - 1u);
+        g.pos_base = r << CB;
+        g.c1 = (int32_t)(r << (CB - 5));
+        g.c2 = (int32_t)(t >> a.log_tpc);
+      }
+    } else {
+      const uint32_t tt = t / a.batch;
+      const uint32_t col = t - tt * a.batch;
+      const uint32_t lbits = a.lo - 5;
+      const uint32_t lchunk = tt & ((1u << lbits) - 1u);
+      g.hb = tt >> lbits;
+      g.pos_base = lchunk << 5;
+      g.s1 = (int32_t)lchunk;
+      g.s3 = (int32_t)g.hb;
+      g.s4 = (int32_t)col;
+    }
+    return g;
+  }
+
+  __device__ static __forceinline__ void tma_load(const CUtensorMap* m, const Geo& g, uint32_t* dst, uint64_t* bar) {
+    if constexpr (KD == Kind::C) tma::load_3d(dst, m, 0, g.c1, g.c2, bar);
+    else tma::load_5d(dst, m, 0, g.s1, 0, g.s3, g.s4, bar);
+  }
+
+  __device__ static __forceinline__ void tma_store(const CUtensorMap* m, const Geo& g, const uint32_t* src) {
+    if constexpr (KD == Kind::C) tma::store_3d(m, 0, g.c1, g.c2, src);
+    else tma::store_5d(m, 0, g.s1, 0, g.s3, g.s4, src);
+  }
+
+  // ---- twiddles: per-layer base pointer + compile-time offset per slot ----
+  template <int k>
+  __device__ static __forceinline__ uint2 twiddle(const TmaArgs& a, const Geo& g, uint32_t ct, int m, int beta) {
+    using M = RM<KD, P, LT, R, k>;
+    const uint32_t cm = M::cm(m);
+    const uint32_t L = a.lo + beta;
+    if constexpr (Net<F, DESC>::kPerPosition) {  // BabyBear: tw[L][pos mod 2^L]
+      const uint2* base = a.tw + ((1u << L) - 1u);
+      if constexpr (KD == Kind::C) {
+        const uint32_t mask = (1u << beta) - 1u;
+        return __ldg(base + ((ct & mask) + (cm & mask)));
+      } else {
+        const uint32_t em = (1u << beta) - 1u;
+        const uint32_t jt = g.pos_base + (ct & 31u) + (((ct >> 5) & em) << a.lo);
+        return __ldg(base + jt + (cm & 31u) + (((cm >> 5) & em) << a.lo));
+      }
+    } else {  // M31: tw[L][pos >> (L+1)]
+      const uint32_t n = 1u << a.log_n;
+      const uint2* base = a.tw + (n - (n >> L));
+      if constexpr (KD == Kind::C) {  // M31 tiles never span columns (tma_pass_ok)
+        return __ldg(base + ((g.pos_base >> (L + 1)) + (ct >> (L + 1)) + (cm >> (L + 1))));
+      } else {
+        return __ldg(base + ((g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1)) + ((cm >> 5) >> (beta + 1))));
+      }
+    }
+  }
+
+  template <int k>
+  __device__ static __forceinline__ void round(uint32_t (&v)[E], const TmaArgs& a, const Geo& g, uint32_t tid) {
+    using M = RM<KD, P, LT, R, k>;
+    constexpr int r = Plan<P, R>::r(k);
+    constexpr int b = Plan<P, R>::b(k);
+    const uint32_t ct = M::ctid(tid);
+#pragma unroll
+    for (int jj = 0; jj < r; ++jj) {
+      const int j = DESC ? (r - 1 - jj) : jj;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        if (m & (1 << j)) continue;
+        butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, g, ct, m, b + j));
+      }
+    }
+  }
+
+  // ---- staging-buffer access in round k's layout ----
+  template <int k>
+  __device__ static constexpr bool vec() {
+    constexpr RoundMap mp = make_map<KD, P, LT, R>(k);
+    return mp.mpos[0] == 0 && mp.mpos[1] == 1;
+  }
+
+  template <int k>
+  __device__ static __forceinline__ void ld(const uint32_t* st, uint32_t (&v)[E], uint32_t tid) {
+    using M = RM<KD, P, LT, R, k>;
+    const uint32_t* p = st + M::ctid(tid);
+    if constexpr (vec<k>()) {
+#pragma unroll
+      for (int m = 0; m < E; m += 4) {
+        const uint4 q = *reinterpret_cast<const uint4*>(p + M::cm(m));
+        v[m] = q.x; v[m + 1] = q.y; v[m + 2] = q.z; v[m + 3] = q.w;
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m) v[m] = p[M::cm(m)];
+    }
+  }
+
+  template <int k>
+  __device__ static __forceinline__ void st(uint32_t* st, const uint32_t (&v)[E], uint32_t tid) {
+    using M = RM<KD, P, LT, R, k>;
+    uint32_t* p = st + M::ctid(tid);
+    if constexpr (vec<k>()) {
+#pragma unroll
+      for (int m = 0; m < E; m += 4)
+        *reinterpret_cast<uint4*>(p + M::cm(m)) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m) p[M::cm(m)] = v[m];
+    }
+  }
+
+  // All K rounds starting from registers in round (DESC ? K-1 : 0)'s layout,
+  // exchanging through `buf`; ends in round (DESC ? 0 : K-1)'s layout.
+  template <int i>
+  __device__ static __forceinline__ void rounds(uint32_t* buf, uint32_t (&v)[E], const TmaArgs& a, const Geo& g,
+                                                uint32_t tid) {
+    if constexpr (i < K) {
+      constexpr int k = DESC ? (K - 1 - i) : i;
+      if constexpr (i > 0) {
+        constexpr int kp = DESC ? (K - i) : (i - 1);
+        st<kp>(buf, v, tid);
+        __syncthreads();
+        ld<k>(buf, v, tid);
+      }
+      round<k>(v, a, g, tid);
+      rounds<i + 1>(buf, v, a, g, tid);
+    }
+  }
+
+  static constexpr int kFirst = DESC ? (K - 1) : 0;
+  static constexpr int kLast = DESC ? 0 : (K - 1);
+
+  __device__ static __forceinline__ void finish(uint32_t (&v)[E], const TmaArgs& a) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      if (a.scale) v[m] = mul_shoup<F>(v[m], a.scale_w, a.scale_ws);
+      else if constexpr (!Net<F, DESC>::kGS) v[m] = reduce2p<F>(v[m]);
+    }
+  }
+
+  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 2 * TWORDS);
+    const uint32_t tid = threadIdx.x;
+    uint32_t t = blockIdx.x;
+    if (t >= a.ntiles) return;
+    if (tid == 0) {
+      tma::prefetch_map(min);
+      tma::prefetch_map(mout);
+      tma::mbar_init(&bar[0], 1);
+      tma::mbar_init(&bar[1], 1);
+      tma::fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tma::mbar_expect_tx(&bar[0], TBYTES);
+      tma_load(min, geo(a, t), stage, &bar[0]);
+    }
+    uint32_t v[E];
+    for (uint32_t it = 0; t < a.ntiles; t += gridDim.x, ++it) {
+      const uint32_t buf = it & 1u;
+      uint32_t* cur = stage + buf * TWORDS;
+      const uint32_t tn = t + gridDim.x;
+      if (tid == 0 && tn < a.ntiles) {
+        tma::wait_reads();  // the store that last used the other buffer has read it
+        tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
+        tma_load(min, geo(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+      }
+      const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(a.err, 1);
+          if (tn < a.ntiles) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          tma::wait_all();
+        }
+        return;
+      }
+      const Geo g = geo(a, t);
+      ld<kFirst>(cur, v, tid);
+      rounds<0>(cur, v, a, g, tid);
+      finish(v, a);
+      st<kLast>(cur, v, tid);
+      tma::fence_proxy_async();
+      __syncthreads();
+      if (tid == 0) {
+        tma_store(mout, g, cur);
+        tma::commit();
+      }
+    }
+    if (tid == 0) tma::wait_all();
+  }
+};
+
+template <class F, bool DESC, Kind KD, int P>
+__global__ void __launch_bounds__(TPass<F, DESC, KD, P>::NT, 2)
+tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
+  TPass<F, DESC, KD, P>::run(&min, &mout, a);
+}
+
+// ---------------------------------------------------------------------------
+// Fused coset-LDE middle step on Kind::S tiles (P <= 8, lo = log_n - P):
+// inverse layers [lo, log_n), then for each output block q the multiplier
+// M_q[pos] (n^-1, coset shift, zero-padded top layers) and forward layers
+// [lo, log_n); block q goes to rows [q n, (q+1) n) of the extended column.
+template <int P>
+struct TExpand {
+  using Inv = TPass<BabyBear, false, Kind::S, P>;
+  using Fwd = TPass<BabyBear, true, Kind::S, P>;
+  static constexpr int K = Inv::K, E = Inv::E, NT = Inv::NT, R = Inv::R, LT = Inv::LT;
+  static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
+
+  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& ai) {
+    extern __shared__ uint8_t smem_raw[];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
+    uint32_t* ostage = stage + 2 * TWORDS;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 3 * TWORDS);
+    const uint32_t tid = threadIdx.x;
+    TmaArgs af = ai;
+    af.tw = ai.tw_fwd;
+    uint32_t t = blockIdx.x;
+    if (t >= ai.ntiles) return;
+    if (tid == 0) {
+      tma::prefetch_map(min);
+      tma::prefetch_map(mout);
+      tma::mbar_init(&bar[0], 1);
+      tma::mbar_init(&bar[1], 1);
+      tma::fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tma::mbar_expect_tx(&bar[0], TBYTES);
+      Inv::tma_load(min, Inv::geo(ai, t), stage, &bar[0]);
+    }
+    using M = RM<Kind::S, P, LT, R, K - 1>;
+    const uint32_t ct = M::ctid(tid);
+    const uint32_t n = 1u << ai.log_n;
+    const uint32_t nq = 1u << ai.log_q;
+    uint32_t x[E], v[E];
+    for (uint32_t it = 0; t < ai.ntiles; t += gridDim.x, ++it) {
+      const uint32_t buf = it & 1u;
+      uint32_t* cur = stage + buf * TWORDS;
+      const uint32_t tn = t + gridDim.x;
+      if (tid == 0 && tn < ai.ntiles) {
+        tma::wait_reads();
+        tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
+        Inv::tma_load(min, Inv::geo(ai, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+      }
+      const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(ai.err, 1);
+          if (tn < ai.ntiles) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          tma::wait_all();
+        }
+        return;
+      }
+      const typename Inv::Geo g = Inv::geo(ai, t);
+      Inv::template ld<0>(cur, x, tid);
+      Inv::template rounds<0>(cur, x, ai, g, tid);  // x: round K-1 layout, values in [0, 2p)
+      // position of slot m: pos_base + u + (e << lo)
+      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << ai.lo);
+      for (uint32_t q = 0; q < nq; ++q) {
+        uint32_t* ob = (q & 1u) ? ostage : cur;
+        if (q >= 2) {  // ob was last used by block q-2's store
+          if (tid == 0) tma::wait_reads_1();
+          __syncthreads();
+        }
+        const uint2* mq = ai.mul + (uint64_t)q * n + pos_t;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << ai.lo));
+          v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
+        }
+        Fwd::template rounds<0>(ob, v, af, g, tid);  // forward starts in round K-1's layout
+        Fwd::template st<0>(ob, v, tid);
+        tma::fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+          tma::store_5d(mout, 0, g.s1, 0, (int32_t)q, g.s4, ob);
+          tma::commit();
+        }
+      }
+    }
+    if (tid == 0) tma::wait_all();
+  }
+};
+
+template <int P>
+__global__ void __launch_bounds__(TExpand<P>::NT, 1)
+tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
+  TExpand<P>::run(&min, &mout, a);
+}
+
+}  // namespace sfntt

@@ -1,0 +1,141 @@
+// tma_launch.cuh -- host side of the persistent TMA tile engine: tensor-map
+// encoding, shape checks and dispatch to the template instantiations.
+#pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <string>
+
+#include "context.hpp"
+#include "tile_tma.cuh"
+
+namespace sfntt {
+
+struct TmaRequest {
+  const uint32_t* in;
+  uint32_t* out;
+  uint64_t in_stride, out_stride;  // column strides in words
+  const uint2* tw;
+  uint32_t log_n, lo;
+  int P;
+  bool contiguous;
+  uint32_t batch;
+  uint32_t scale_w;  // canonical multiplier for the outputs; 0 = none
+};
+
+// Resolved once through the runtime (no link-time dependency on libcuda).
+Status tensor_map_encode(CUtensorMap* map, const void* base, uint32_t rank, const cuuint64_t* dims,
+                         const cuuint64_t* strides_bytes, const cuuint32_t* box);
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Can a pass of this shape run on the TMA engine?  (Per-block M31 twiddles
+// are only supported on tiles inside one column.)
+inline bool tma_pass_ok(const TmaRequest& r, bool per_block) {
+  if (!aligned16(r.in) || !aligned16(r.out) || (r.in_stride & 3) || (r.out_stride & 3)) return false;
+  const uint64_t n = 1ull << r.log_n;
+  if (r.contiguous) {
+    if (r.P < 5 || r.P > 12 || r.lo != 0) return false;
+    if (n >= kTileWords) return true;
+    return !per_block && r.in_stride == n && r.out_stride == n && ((uint64_t)r.batch * n) % kTileWords == 0;
+  }
+  return r.P >= 1 && r.P <= 8 && r.lo >= 5 && r.lo + r.P <= r.log_n;
+}
+
+inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n, uint64_t stride, uint32_t batch) {
+  const uint64_t n = 1ull << log_n;
+  cuuint64_t dims[3], strides[2];
+  const cuuint32_t box[3] = {32, kTileWords / 32, 1};
+  if (n >= kTileWords) {
+    dims[0] = 32; dims[1] = n / 32; dims[2] = batch;
+    strides[0] = 128; strides[1] = stride * 4;
+  } else {
+    dims[0] = 32; dims[1] = (uint64_t)batch * n / 32; dims[2] = 1;
+    strides[0] = 128; strides[1] = (uint64_t)batch * n * 4;
+  }
+  return tensor_map_encode(m, base, 3, dims, strides, box);
+}
+
+// column viewed as [hb][e][lchunk][u]: u 32 words, lchunk 2^lo/32, e 2^P (stride 2^lo), hb
+inline Status encode_s_map(CUtensorMap* m, const uint32_t* base, uint32_t lo, int P, uint64_t hb_count,
+                           uint64_t hb_stride, uint64_t stride, uint32_t batch) {
+  const cuuint64_t dims[5] = {32, (1ull << lo) / 32, 1ull << P, hb_count, batch};
+  const cuuint64_t strides[4] = {128, (1ull << lo) * 4, hb_stride * 4, stride * 4};
+  const cuuint32_t box[5] = {32, 1, (cuuint32_t)(1u << P), 1, 1};
+  return tensor_map_encode(m, base, 5, dims, strides, box);
+}
+
+template <class F, bool DESC, Kind KD, int P>
+const char* tma_pass_name() {
+  static const std::string nm = std::string(F::kMontgomery ? "bb_" : "m31_") + (DESC ? "fwd" : "inv") +
+                                "_tma_" + (KD == Kind::C ? "C" : "S") + std::to_string(P);
+  return nm.c_str();
+}
+
+template <class F, bool DESC, Kind KD, int P>
+Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
+  using T = TPass<F, DESC, KD, P>;
+  const uint64_t n = 1ull << r.log_n;
+  CUtensorMap min, mout;
+  TmaArgs a{};
+  a.tw = r.tw;
+  a.log_n = r.log_n;
+  a.lo = r.lo;
+  a.batch = r.batch;
+  a.err = ctx->err.as<int>();
+  a.scale = r.scale_w ? 1u : 0u;
+  a.scale_w = r.scale_w;
+  a.scale_ws = (uint32_t)(((uint64_t)r.scale_w << 32) / F::P);
+  if constexpr (KD == Kind::C) {
+    SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch));
+    SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch));
+    a.spans = n < kTileWords;
+    a.log_tpc = a.spans ? 0u : r.log_n - kTileBits;
+    a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> kTileBits);
+  } else {
+    const uint64_t hb = n >> (r.lo + P);
+    SFNTT_TRY(encode_s_map(&min, r.in, r.lo, P, hb, 1ull << (r.lo + P), r.in_stride, r.batch));
+    SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
+    a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
+  }
+  constexpr int smem = 2 * (int)T::TBYTES + 16 + 1024;
+  auto kern = tma_pass_kernel<F, DESC, KD, P>;
+  SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, 2u * (uint32_t)ctx->sm_count);
+  launch_begin(ctx, s);
+  kern<<<grid, T::NT, smem, s>>>(min, mout, a);
+  return launch_check(ctx, tma_pass_name<F, DESC, KD, P>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
+}
+
+#define SFNTT_TMA_C(PP) \
+  case PP: return launch_tma_pass<F, DESC, Kind::C, PP>(ctx, r, s);
+#define SFNTT_TMA_S(PP) \
+  case PP: return launch_tma_pass<F, DESC, Kind::S, PP>(ctx, r, s);
+
+template <class F, bool DESC>
+Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
+  if (!tma_pass_ok(r, !F::kMontgomery)) return {SFNTT_INVALID_ARGUMENT, "pass shape not supported by the TMA engine"};
+  if (r.contiguous) {
+    switch (r.P) {
+      SFNTT_TMA_C(5) SFNTT_TMA_C(6) SFNTT_TMA_C(7) SFNTT_TMA_C(8)
+      SFNTT_TMA_C(9) SFNTT_TMA_C(10) SFNTT_TMA_C(11) SFNTT_TMA_C(12)
+      default: break;
+    }
+  } else {
+    switch (r.P) {
+      SFNTT_TMA_S(1) SFNTT_TMA_S(2) SFNTT_TMA_S(3) SFNTT_TMA_S(4)
+      SFNTT_TMA_S(5) SFNTT_TMA_S(6) SFNTT_TMA_S(7) SFNTT_TMA_S(8)
+      default: break;
+    }
+  }
+  return {SFNTT_INVALID_ARGUMENT, "unsupported TMA pass size"};
+}
+#undef SFNTT_TMA_C
+#undef SFNTT_TMA_S
+
+Status run_tma_pass_bb_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+Status run_tma_pass_bb_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+Status run_tma_pass_m31_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+Status run_tma_pass_m31_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+
+}  // namespace sfntt

@@ -43,6 +43,7 @@ SIGNATURES = {
     "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
     "sfntt_host_free": (i32, [vp, vp]),
     "sfntt_launch_count": (u64, [vp]),
+    "sfntt_check_device_error": (i32, [vp]),
     "sfntt_kernel_timing": (i32, [vp, i32]),
     "sfntt_kernel_times": (i32, [vp, ctypes.c_char_p, sz]),
 }
