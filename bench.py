@@ -277,6 +277,18 @@ def main() -> None:
     kernels = {k: {"launches": v[0], "avg_ms": v[1] / v[0], "share": v[1] / sum(t[1] for t in kt.values()),
                    "gbs": (v[2] / v[0]) / (v[1] / v[0] * 1e-3) / 1e9} for k, v in kt.items()}
     lde_gbs = algorithmic_bytes(a) / (step_ms * 1e-3) / 1e9
+    # integer roofline: radix-2 butterflies of the LDE (the zero-padded top
+    # added_bits layers are multiplications only) against the measured
+    # register-resident butterfly rate of this GPU
+    bf_peak = {"gs": ctx.butterfly_peak(True), "ct": ctx.butterfly_peak(False)}
+    lde_bf = a.batch * ((n // 2) * a.log_n + (n_ext // 2) * a.log_n)
+    dom_bf = kernel_butterflies(name, nbytes // nl, a.added_bits)
+    int_roofline = {"bound": "int32 issue", "unit": "butterflies/s",
+                    "peak": bf_peak["gs"], "peak_ct": bf_peak["ct"],
+                    "peak_kind": "measured on this GPU (sfntt_butterfly_peak, register-resident butterflies)",
+                    "lde_achieved": lde_bf / (step_ms * 1e-3), "lde_frac": lde_bf / (step_ms * 1e-3) / bf_peak["gs"],
+                    "kernel": name, "kernel_achieved": dom_bf / (avg_ms * 1e-3),
+                    "kernel_frac": dom_bf / (avg_ms * 1e-3) / bf_peak["gs"]}
 
     # end to end through the host-buffer C-ABI call (copies inside the timed region)
     e2e = None
@@ -318,9 +330,23 @@ def main() -> None:
             "gpu_launches": launches, "launches_per_step": launches / a.steps,
             "lde_gbs": lde_gbs, "lde_hbm_frac": lde_gbs / peak,
             "melem_per_s_out": a.batch * n_ext / (value * 1e-3) / 1e6,
-            "roofline": roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu,
+            "roofline": roofline, "int_roofline": int_roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e,
+            "cpu_baseline": cpu,
             "secondary": secondary, "device": ctx.device_info()}
     print(json.dumps(line), flush=True)
+
+
+def kernel_butterflies(name: str, bytes_per_launch: int, added_bits: int) -> float:
+    """Radix-2 butterflies of one launch, from its label and algorithmic bytes
+    (pass kernels move each point once each way; the expand reads a tile and
+    writes 2^added_bits blocks, running P layers on the input and on every block)."""
+    import re
+    m = re.search(r"_([CS])(\d+)", name)
+    layers = int(m.group(2)) if m else 1
+    if "expand" in name:
+        elems_in = bytes_per_launch / (4 * (1 + (1 << added_bits)))
+        return elems_in / 2 * layers * (1 + (1 << added_bits))
+    return bytes_per_launch / 8 / 2 * layers
 
 
 def secondary_metrics(ctx, sfntt, torch) -> dict:

@@ -160,6 +160,13 @@ uint64_t sfntt_launch_count(const sfntt_ctx *ctx);
 int sfntt_kernel_timing(sfntt_ctx *ctx, int enable);
 int sfntt_kernel_times(sfntt_ctx *ctx, char *buf, size_t len);
 
+/* Measured integer ceiling: radix-2 butterflies per second this GPU sustains
+ * with register-resident data (gs = 1: GS on canonical values, the forward
+ * butterfly; gs = 0: lazy CT, the inverse one).  The NTT passes are bound by
+ * 32-bit integer issue, so the bench reports their fraction of this beside
+ * the HBM roofline.  No reference counterpart. */
+int sfntt_butterfly_peak(sfntt_ctx *ctx, int gs, double *butterflies_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,6 +78,13 @@ struct DevBuf {
 
 }  // namespace sfntt
 
+#ifndef SFNTT_NTT_PLAIN_DEFAULT
+#define SFNTT_NTT_PLAIN_DEFAULT true
+#endif
+#ifndef SFNTT_LDE_PLAIN_DEFAULT
+#define SFNTT_LDE_PLAIN_DEFAULT false
+#endif
+
 struct sfntt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;         // host-memory calls run here
@@ -102,6 +109,11 @@ struct sfntt_ctx {
   sfntt::DevBuf err;
   // route every pass through the first (non-TMA) tile engine (tests / A-B)
   bool no_tma = false;
+  // BabyBear strided passes: plain sub-transforms + four-step twists applied by
+  // neighbouring passes (true) or per-position twiddles (false); separately
+  // for plain NTTs and the fused LDE.
+  bool ntt_plain = SFNTT_NTT_PLAIN_DEFAULT;
+  bool lde_plain = SFNTT_LDE_PLAIN_DEFAULT;
 
   // Opt-in per-kernel timing (sfntt_kernel_timing): an event pair around every
   // launch, resolved and aggregated by name in sfntt_kernel_times.
@@ -122,14 +134,23 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
 Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty, int kind,
                     cudaStream_t stream, const uint2** out);
 
+// Twist of a strided BabyBear pass over layers [lo, lo + P), indexed by
+// column position mod 2^(lo+P) (cached like the LDE tables).
+Status bb_twist_table(sfntt_ctx* ctx, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream, const uint2** out);
+
 // Kernel drivers (ntt.cu / lde.cu / elementwise.cu)
 Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d_data, uint32_t log_n,
                uint32_t batch, cudaStream_t stream);
 // Layers [a, b) of a 2^log_n network on `batch` columns (first pass in -> out,
 // later passes in place); scale_w != 0 multiplies the final outputs.
+// edge_twist (BabyBear, TMA engine only): a four-step twist applied to the
+// inputs of a forward range or the outputs of an inverse range, indexed by
+// column position & edge_mask -- the boundary with an adjacent strided pass
+// run by another kernel.
 Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
                   uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
-                  const uint2* tw, cudaStream_t stream);
+                  const uint2* tw, cudaStream_t stream, const uint2* edge_twist = nullptr,
+                  uint32_t edge_mask = 0);
 Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in, uint32_t* d_out,
                    uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize,
                    cudaStream_t stream);

@@ -173,11 +173,11 @@ __global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, 
   }
 }
 
-template <int P>
+template <int P, bool PLAIN>
 Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_stride, uint32_t* d_out, uint32_t log_n,
                          uint32_t batch, uint32_t added_bits, const uint2* tw_inv, const uint2* tw_fwd,
                          const uint2* mul, cudaStream_t s) {
-  using X = TExpand<P>;
+  using X = TExpand<P, PLAIN>;
   const uint32_t lo = log_n - P;
   const uint64_t n = 1ull << log_n, n_ext = n << added_bits;
   CUtensorMap min, mout;
@@ -193,13 +193,13 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   a.log_q = added_bits;
   a.err = ctx->err.as<int>();
   a.ntiles = (uint32_t)(((uint64_t)batch * n) >> (P + 5));
-  constexpr int smem = 3 * (int)X::TBYTES + 16 + 1024;
-  auto kern = tma_expand_kernel<P>;
+  constexpr int smem = 3 * (int)X::TBYTES + 16 + 16 * (int)X::Inv::TW_ENTRIES + 1024;
+  auto kern = tma_expand_kernel<P, PLAIN>;
   SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, X::NT, smem, s>>>(min, mout, a);
-  static const std::string name = "bb_lde_expand_tma_S" + std::to_string(P);
+  static const std::string name = "bb_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "");
   return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
 }
 
@@ -220,13 +220,27 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
     SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 0, s, &mul));
     const bool tma_ok = !ctx->no_tma && log_n >= 13 && aligned16(d_in) && aligned16(d_out);
     if (tma_ok) {
-      // I1: inverse layers [0, log_n - 8) into the output buffer; X: the
-      // persistent TMA expand on 8-layer strided tiles; F3: forward [0, lo).
+      // I1: inverse layers [0, lo) into the output buffer, ending with the
+      // four-step pre-twist of the expand's sub-iDFT; X: the persistent TMA
+      // expand on 8-layer strided tiles (plain sub-transforms); F3: forward
+      // layers [0, lo) of the n_ext network, starting with the expand's
+      // post-twist (the same for every output block, so indexed mod n).
       const uint32_t lo = log_n - 8;
-      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s));
-      SFNTT_TRY(launch_tma_expand<8>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s));
+      const uint2 *tw_i = nullptr, *tw_f = nullptr;
+      const bool plain = ctx->lde_plain;
+      if (plain) {
+        SFNTT_TRY(bb_twist_table(ctx, lo, 8, true, s, &tw_i));
+        SFNTT_TRY(bb_twist_table(ctx, lo, 8, false, s, &tw_f));
+      }
+      const uint32_t mask = (uint32_t)(n - 1);
+      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s,
+                           tw_i, mask));
+      if (plain)
+        SFNTT_TRY((launch_tma_expand<8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s)));
+      else
+        SFNTT_TRY((launch_tma_expand<8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s)));
       SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd,
-                           s));
+                           s, tw_f, mask));
       return {};
     }
     const uint32_t lo = log_n <= 12 ? 0u : (log_n + 1) / 2;

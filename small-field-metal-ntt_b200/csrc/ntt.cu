@@ -62,7 +62,7 @@ static uint32_t inv_n_canonical(int field, uint32_t log_n) {
 // output of the last pass by the canonical constant scale_w.
 Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
                   uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
-                  const uint2* tw, cudaStream_t s) {
+                  const uint2* tw, cudaStream_t s, const uint2* edge_twist, uint32_t edge_mask) {
   uint32_t lo[4], cnt[4];
   if (!ctx->no_tma) {
     const int kt = tma_split(a, b, lo, cnt);
@@ -84,11 +84,33 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
       r.scale_w = (i == kt - 1) ? scale_w : 0u;
       ok = tma_pass_ok(r, field == SFNTT_M31);
     }
+    if (ok && field == SFNTT_BABYBEAR) {
+      // Strided passes either use per-position twiddles (self-contained) or,
+      // when `plain`, run plain sub-transforms whose four-step twist is applied
+      // by a neighbour: forward -> the next pass at its load, inverse -> the
+      // previous pass at its store.  The edge twist of the whole range goes to
+      // its first (forward) / last (inverse) pass.
+      const bool plain = ctx->ntt_plain;
+      for (int i = 0; i < kt; ++i) {
+        const int pi = inverse ? i : (kt - 1 - i);
+        req[i].plain = plain && !req[i].contiguous;
+        if ((!inverse && i == 0) || (inverse && i == kt - 1)) {
+          req[i].twist = edge_twist;
+          req[i].twist_mask = edge_mask;
+          continue;
+        }
+        if (!plain) continue;
+        const int nb = pi + 1;  // the strided chunk just above pi
+        SFNTT_TRY(bb_twist_table(ctx, lo[nb], cnt[nb], inverse, s, &req[i].twist));
+        req[i].twist_mask = (1u << (lo[nb] + cnt[nb])) - 1u;
+      }
+    }
     if (ok) {
       for (int i = 0; i < kt; ++i) SFNTT_TRY(run_tma_pass(ctx, field, !inverse, req[i], s));
       return {};
     }
   }
+  if (edge_twist) return {SFNTT_INVALID_ARGUMENT, "a boundary twist needs the TMA engine"};
   const int k = split_layers(a, b, lo, cnt);
   const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
   for (int i = 0; i < k; ++i) {

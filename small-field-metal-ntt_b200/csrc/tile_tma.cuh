@@ -38,11 +38,22 @@ struct TmaArgs {
   uint32_t spans;      // Kind::C: tiles span columns (n < 2^13, dense columns)
   uint32_t scale, scale_w, scale_ws;
   int* err;
+  // four-step twist applied at this pass's boundary (BabyBear): forward
+  // passes multiply their inputs, inverse passes their outputs, by
+  // twist[pos & twist_mask]; nullptr = none
+  const uint2* twist;
+  uint32_t twist_mask;
   // fused LDE expansion (Expand kernel only)
   const uint2* tw_fwd;
   const uint2* mul;
   uint32_t log_q;
 };
+
+// The forward half of the LDE expansion reads the forward twiddle table.
+struct FwdArgs : TmaArgs {
+  __device__ explicit FwdArgs(const TmaArgs& a) : TmaArgs(a) { tw = a.tw_fwd; }
+};
+__device__ __forceinline__ FwdArgs fwd_args(const TmaArgs& a) { return FwdArgs(a); }
 
 // Where a tile sits: tensor-map coordinates and the column position of its
 // first word (shared by every pass type so fused kernels can mix directions).
@@ -53,7 +64,12 @@ struct TileCoord {
   int32_t s1, s3, s4; // Kind::S map coordinates (lchunk, hb, column)
 };
 
-template <class F, bool DESC, Kind KD, int P>
+// PLAIN (BabyBear Kind::S only): run the plain 2^P-point sub-transform with
+// lane-independent twiddles from shared memory and leave the four-step twist to
+// the neighbouring pass; otherwise use the reference's per-position twiddles
+// tw[L][pos mod 2^L] from the global table.  TW: this pass applies a boundary
+// twist (forward: at load, inverse: at store).
+template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false>
 struct TPass {
   static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
   static constexpr int CB = P + LT;
@@ -104,22 +120,31 @@ struct TPass {
     else tma::store_5d(m, 0, g.s1, 0, g.s3, g.s4, src);
   }
 
+  // BabyBear passes read their twiddles from a shared-memory copy of layers
+  // [0, P) of the global table: contiguous passes need tw[L][pos mod 2^L]
+  // with L < P; strided passes run the plain 2^P-point sub-transform, whose
+  // layer-beta twiddle tw[beta][e mod 2^beta] is the same for every lane (the
+  // per-position remainder is the boundary twist).
+  static constexpr bool kStaged = F::kMontgomery && (KD == Kind::C || PLAIN);
+  static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
+
   // ---- twiddles: per-layer base pointer + compile-time offset per slot ----
   template <int k>
-  __device__ static __forceinline__ uint2 twiddle(const TmaArgs& a, const Geo& g, uint32_t ct, int m, int beta) {
+  __device__ static __forceinline__ uint2 twiddle(const TmaArgs& a, const uint2* tws, const Geo& g, uint32_t ct, int m,
+                                                  int beta) {
     using M = RM<KD, P, LT, R, k>;
     const uint32_t cm = M::cm(m);
     const uint32_t L = a.lo + beta;
-    if constexpr (Net<F, DESC>::kPerPosition) {  // BabyBear: tw[L][pos mod 2^L]
+    if constexpr (kStaged) {
+      const uint2* base = tws + ((1u << beta) - 1u);
+      const uint32_t mask = (1u << beta) - 1u;
+      if constexpr (KD == Kind::C) return base[(ct & mask) + (cm & mask)];
+      else return base[((ct >> 5) & mask) + ((cm >> 5) & mask)];
+    } else if constexpr (F::kMontgomery) {  // BabyBear strided, per position: tw[L][pos mod 2^L]
       const uint2* base = a.tw + ((1u << L) - 1u);
-      if constexpr (KD == Kind::C) {
-        const uint32_t mask = (1u << beta) - 1u;
-        return __ldg(base + ((ct & mask) + (cm & mask)));
-      } else {
-        const uint32_t em = (1u << beta) - 1u;
-        const uint32_t jt = g.pos_base + (ct & 31u) + (((ct >> 5) & em) << a.lo);
-        return __ldg(base + jt + (cm & 31u) + (((cm >> 5) & em) << a.lo));
-      }
+      const uint32_t em = (1u << beta) - 1u;
+      const uint32_t jt = g.pos_base + (ct & 31u) + (((ct >> 5) & em) << a.lo);
+      return __ldg(base + jt + (cm & 31u) + (((cm >> 5) & em) << a.lo));
     } else {  // M31: tw[L][pos >> (L+1)]
       const uint32_t n = 1u << a.log_n;
       const uint2* base = a.tw + (n - (n >> L));
@@ -132,7 +157,8 @@ struct TPass {
   }
 
   template <int k>
-  __device__ static __forceinline__ void round(uint32_t (&v)[E], const TmaArgs& a, const Geo& g, uint32_t tid) {
+  __device__ static __forceinline__ void round(uint32_t (&v)[E], const TmaArgs& a, const uint2* tws, const Geo& g,
+                                               uint32_t tid) {
     using M = RM<KD, P, LT, R, k>;
     constexpr int r = Plan<P, R>::r(k);
     constexpr int b = Plan<P, R>::b(k);
@@ -143,7 +169,7 @@ struct TPass {
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         if (m & (1 << j)) continue;
-        butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, g, ct, m, b + j));
+        butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, tws, g, ct, m, b + j));
       }
     }
   }
@@ -188,8 +214,8 @@ struct TPass {
   // All K rounds starting from registers in round (DESC ? K-1 : 0)'s layout,
   // exchanging through `buf`; ends in round (DESC ? 0 : K-1)'s layout.
   template <int i>
-  __device__ static __forceinline__ void rounds(uint32_t* buf, uint32_t (&v)[E], const TmaArgs& a, const Geo& g,
-                                                uint32_t tid) {
+  __device__ static __forceinline__ void rounds(uint32_t* buf, uint32_t (&v)[E], const TmaArgs& a, const uint2* tws,
+                                                const Geo& g, uint32_t tid) {
     if constexpr (i < K) {
       constexpr int k = DESC ? (K - 1 - i) : i;
       if constexpr (i > 0) {
@@ -198,30 +224,60 @@ struct TPass {
         __syncthreads();
         ld<k>(buf, v, tid);
       }
-      round<k>(v, a, g, tid);
-      rounds<i + 1>(buf, v, a, g, tid);
+      round<k>(v, a, tws, g, tid);
+      rounds<i + 1>(buf, v, a, tws, g, tid);
     }
   }
 
   static constexpr int kFirst = DESC ? (K - 1) : 0;
   static constexpr int kLast = DESC ? 0 : (K - 1);
 
-  __device__ static __forceinline__ void finish(uint32_t (&v)[E], const TmaArgs& a) {
+  // column position of slot m in round k's layout
+  template <int k>
+  __device__ static __forceinline__ uint32_t pos_of(const TmaArgs& a, const Geo& g, uint32_t ct, int m) {
+    using M = RM<KD, P, LT, R, k>;
+    const uint32_t cm = M::cm(m);
+    if constexpr (KD == Kind::C) return g.pos_base + ct + cm;
+    else
+      return (g.hb << (a.lo + P)) + g.pos_base + (ct & 31u) + (cm & 31u) + (((ct >> 5) + (cm >> 5)) << a.lo);
+  }
+
+  template <int k>
+  __device__ static __forceinline__ void twist(uint32_t (&v)[E], const TmaArgs& a, const Geo& g, uint32_t tid) {
+    using M = RM<KD, P, LT, R, k>;
+    const uint32_t ct = M::ctid(tid);
 #pragma unroll
     for (int m = 0; m < E; ++m) {
-      if (a.scale) v[m] = mul_shoup<F>(v[m], a.scale_w, a.scale_ws);
-      else if constexpr (!Net<F, DESC>::kGS) v[m] = reduce2p<F>(v[m]);
+      const uint2 w = __ldg(a.twist + (pos_of<k>(a, g, ct, m) & a.twist_mask));
+      v[m] = mul_shoup<F>(v[m], w.x, w.y);
     }
   }
 
-  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& a) {
+  __device__ static __forceinline__ void finish(uint32_t (&v)[E], const TmaArgs& a, const Geo& g, uint32_t tid) {
+    if constexpr (!DESC && TW) twist<kLast>(v, a, g, tid);  // canonical afterwards
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      if (a.scale) v[m] = mul_shoup<F>(v[m], a.scale_w, a.scale_ws);
+      else if constexpr (!Net<F, DESC>::kGS && (DESC || !TW)) v[m] = reduce2p<F>(v[m]);
+    }
+  }
+
+  // Copy the twiddle layers [0, P) into shared memory (BabyBear).
+  __device__ static __forceinline__ void stage_twiddles(uint2* dst, const uint2* src, uint32_t tid) {
+    for (uint32_t i = tid; i < TW_ENTRIES; i += NT) dst[i] = __ldg(src + i);
+  }
+
+  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     extern __shared__ uint8_t smem_raw[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
     uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 2 * TWORDS);
+    uint2* tws = reinterpret_cast<uint2*>(bar + 2);
     const uint32_t tid = threadIdx.x;
+    const TmaArgs& a = args;
     uint32_t t = blockIdx.x;
     if (t >= a.ntiles) return;
+    if constexpr (kStaged) stage_twiddles(tws, a.tw, tid);
     if (tid == 0) {
       tma::prefetch_map(min);
       tma::prefetch_map(mout);
@@ -255,8 +311,9 @@ struct TPass {
       }
       const Geo g = geo(a, t);
       ld<kFirst>(cur, v, tid);
-      rounds<0>(cur, v, a, g, tid);
-      finish(v, a);
+      if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
+      rounds<0>(cur, v, a, tws, g, tid);
+      finish(v, a, g, tid);
       st<kLast>(cur, v, tid);
       tma::fence_proxy_async();
       __syncthreads();
@@ -269,10 +326,10 @@ struct TPass {
   }
 };
 
-template <class F, bool DESC, Kind KD, int P>
-__global__ void __launch_bounds__(TPass<F, DESC, KD, P>::NT, 2)
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
+__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW>::NT, 2)
 tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
-  TPass<F, DESC, KD, P>::run(&min, &mout, a);
+  TPass<F, DESC, KD, P, PLAIN, TW>::run(&min, &mout, a);
 }
 
 // ---------------------------------------------------------------------------
@@ -280,24 +337,29 @@ tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__
 // inverse layers [lo, log_n), then for each output block q the multiplier
 // M_q[pos] (n^-1, coset shift, zero-padded top layers) and forward layers
 // [lo, log_n); block q goes to rows [q n, (q+1) n) of the extended column.
-template <int P>
+template <int P, bool PLAIN>
 struct TExpand {
-  using Inv = TPass<BabyBear, false, Kind::S, P>;
-  using Fwd = TPass<BabyBear, true, Kind::S, P>;
+  using Inv = TPass<BabyBear, false, Kind::S, P, PLAIN>;
+  using Fwd = TPass<BabyBear, true, Kind::S, P, PLAIN>;
   static constexpr int K = Inv::K, E = Inv::E, NT = Inv::NT, R = Inv::R, LT = Inv::LT;
   static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
 
-  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& ai) {
+  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     extern __shared__ uint8_t smem_raw[];
     uint32_t* stage = reinterpret_cast<uint32_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
     uint32_t* ostage = stage + 2 * TWORDS;
     uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 3 * TWORDS);
+    uint2* tws_inv = reinterpret_cast<uint2*>(bar + 2);
+    uint2* tws_fwd = tws_inv + Inv::TW_ENTRIES;
     const uint32_t tid = threadIdx.x;
-    TmaArgs af = ai;
-    af.tw = ai.tw_fwd;
+    const TmaArgs& ai = args;
     uint32_t t = blockIdx.x;
     if (t >= ai.ntiles) return;
+    if constexpr (PLAIN) {
+      Inv::stage_twiddles(tws_inv, ai.tw, tid);
+      Fwd::stage_twiddles(tws_fwd, ai.tw_fwd, tid);
+    }
     if (tid == 0) {
       tma::prefetch_map(min);
       tma::prefetch_map(mout);
@@ -335,7 +397,7 @@ struct TExpand {
       }
       const typename Inv::Geo g = Inv::geo(ai, t);
       Inv::template ld<0>(cur, x, tid);
-      Inv::template rounds<0>(cur, x, ai, g, tid);  // x: round K-1 layout, values in [0, 2p)
+      Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout, values in [0, 2p)
       // position of slot m: pos_base + u + (e << lo)
       const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << ai.lo);
       for (uint32_t q = 0; q < nq; ++q) {
@@ -350,7 +412,7 @@ struct TExpand {
           const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << ai.lo));
           v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
         }
-        Fwd::template rounds<0>(ob, v, af, g, tid);  // forward starts in round K-1's layout
+        Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, g, tid);  // forward starts in round K-1's layout
         Fwd::template st<0>(ob, v, tid);
         tma::fence_proxy_async();
         __syncthreads();
@@ -364,10 +426,10 @@ struct TExpand {
   }
 };
 
-template <int P>
-__global__ void __launch_bounds__(TExpand<P>::NT, 1)
+template <int P, bool PLAIN>
+__global__ void __launch_bounds__(TExpand<P, PLAIN>::NT, 1)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
-  TExpand<P>::run(&min, &mout, a);
+  TExpand<P, PLAIN>::run(&min, &mout, a);
 }
 
 }  // namespace sfntt

@@ -21,6 +21,9 @@ struct TmaRequest {
   bool contiguous;
   uint32_t batch;
   uint32_t scale_w;  // canonical multiplier for the outputs; 0 = none
+  const uint2* twist = nullptr;  // BabyBear four-step twist at the boundary
+  uint32_t twist_mask = 0;
+  bool plain = false;            // BabyBear strided pass: plain sub-transform (twist by neighbours)
 };
 
 // Resolved once through the runtime (no link-time dependency on libcuda).
@@ -65,16 +68,17 @@ inline Status encode_s_map(CUtensorMap* m, const uint32_t* base, uint32_t lo, in
   return tensor_map_encode(m, base, 5, dims, strides, box);
 }
 
-template <class F, bool DESC, Kind KD, int P>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
 const char* tma_pass_name() {
   static const std::string nm = std::string(F::kMontgomery ? "bb_" : "m31_") + (DESC ? "fwd" : "inv") +
-                                "_tma_" + (KD == Kind::C ? "C" : "S") + std::to_string(P);
+                                "_tma_" + (KD == Kind::C ? "C" : "S") + std::to_string(P) + (PLAIN ? "p" : "") +
+                                (TW ? "t" : "");
   return nm.c_str();
 }
 
-template <class F, bool DESC, Kind KD, int P>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
 Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
-  using T = TPass<F, DESC, KD, P>;
+  using T = TPass<F, DESC, KD, P, PLAIN, TW>;
   const uint64_t n = 1ull << r.log_n;
   CUtensorMap min, mout;
   TmaArgs a{};
@@ -86,6 +90,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   a.scale = r.scale_w ? 1u : 0u;
   a.scale_w = r.scale_w;
   a.scale_ws = (uint32_t)(((uint64_t)r.scale_w << 32) / F::P);
+  a.twist = r.twist;
+  a.twist_mask = r.twist_mask;
   if constexpr (KD == Kind::C) {
     SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch));
     SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch));
@@ -98,23 +104,35 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
   }
-  constexpr int smem = 2 * (int)T::TBYTES + 16 + 1024;
-  auto kern = tma_pass_kernel<F, DESC, KD, P>;
+  constexpr int smem = 2 * (int)T::TBYTES + 16 + 8 * (int)T::TW_ENTRIES + 1024;
+  auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW>;
   SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, 2u * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, T::NT, smem, s>>>(min, mout, a);
-  return launch_check(ctx, tma_pass_name<F, DESC, KD, P>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
+  return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
 }
 
-#define SFNTT_TMA_C(PP) \
-  case PP: return launch_tma_pass<F, DESC, Kind::C, PP>(ctx, r, s);
-#define SFNTT_TMA_S(PP) \
-  case PP: return launch_tma_pass<F, DESC, Kind::S, PP>(ctx, r, s);
+// BabyBear instantiates the twist / plain variants; M31 never needs them.
+#define SFNTT_TMA_C(PP)                                                                          \
+  case PP:                                                                                       \
+    if constexpr (F::kMontgomery) {                                                              \
+      if (r.twist) return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);         \
+    }                                                                                            \
+    return launch_tma_pass<F, DESC, Kind::C, PP, false, false>(ctx, r, s);
+#define SFNTT_TMA_S(PP)                                                                          \
+  case PP:                                                                                       \
+    if constexpr (F::kMontgomery) {                                                              \
+      if (r.plain && r.twist) return launch_tma_pass<F, DESC, Kind::S, PP, true, true>(ctx, r, s); \
+      if (r.plain) return launch_tma_pass<F, DESC, Kind::S, PP, true, false>(ctx, r, s);         \
+      if (r.twist) return launch_tma_pass<F, DESC, Kind::S, PP, false, true>(ctx, r, s);         \
+    }                                                                                            \
+    return launch_tma_pass<F, DESC, Kind::S, PP, false, false>(ctx, r, s);
 
 template <class F, bool DESC>
 Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   if (!tma_pass_ok(r, !F::kMontgomery)) return {SFNTT_INVALID_ARGUMENT, "pass shape not supported by the TMA engine"};
+  if (!F::kMontgomery && (r.twist || r.plain)) return {SFNTT_INVALID_ARGUMENT, "M31 passes take no twist"};
   if (r.contiguous) {
     switch (r.P) {
       SFNTT_TMA_C(5) SFNTT_TMA_C(6) SFNTT_TMA_C(7) SFNTT_TMA_C(8)

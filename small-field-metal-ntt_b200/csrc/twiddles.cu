@@ -84,6 +84,22 @@ __global__ void bb_power_table_kernel(uint2* tab, uint32_t log_len, uint32_t cou
   tab[t] = make_uint2(w, shoup_of<BabyBear>(w));
 }
 
+// Four-step twist of a strided pass over layers [lo, lo + P) (span N =
+// 2^(lo+P)): tab[pos] = g_N^(+-(pos mod 2^lo) * rev_P(pos >> lo)).  The
+// reference's per-position DIF layers equal the plain 2^P-point sub-DIF
+// followed by this factor, and its DIT layers equal the plain sub-DIT applied
+// to inputs multiplied by the inverse factor.
+__global__ void bb_twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_monty) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (1u << (lo + P))) return;
+  const uint32_t l = t & ((1u << lo) - 1u);
+  const uint32_t e = t >> lo;
+  const uint32_t re = __brev(e) >> (32u - P);
+  uint32_t w = pow_var<BabyBear>(g_monty, l * re);
+  w = to_canonical(BabyBear{}, w);
+  tab[t] = make_uint2(w, shoup_of<BabyBear>(w));
+}
+
 Status sync_after_build(sfntt_ctx* ctx, cudaStream_t stream, const char* what) {
   SFNTT_TRY(launch_check(ctx, what));
   SFNTT_CU(cudaStreamSynchronize(stream));
@@ -173,6 +189,30 @@ Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_
     SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
     bb_power_table_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_len, count, B, scale);
     Status s = sync_after_build(ctx, stream, "bb_power_table_kernel");
+    if (!s.ok()) { buf.release(); return s; }
+    it = ctx->lde_tabs.emplace(key, buf).first;
+  }
+  *out = it->second.as<uint2>();
+  return {};
+}
+
+}  // namespace sfntt
+
+namespace sfntt {
+
+Status bb_twist_table(sfntt_ctx* ctx, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream, const uint2** out) {
+  if (lo + P > host::BB_TWO_ADICITY || P == 0 || P > 8) return {SFNTT_INVALID_ARGUMENT, "twist span"};
+  const auto key = std::make_tuple(lo, P, inverse ? 1u : 0u, 2);
+  auto it = ctx->lde_tabs.find(key);
+  if (it == ctx->lde_tabs.end()) {
+    if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twist table not prepared before capture"};
+    uint32_t g = host::bb_two_adic_generator(lo + P);
+    if (inverse) g = host::invmod(g, host::BB_P);
+    const uint32_t count = 1u << (lo + P);
+    DevBuf buf;
+    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    bb_twist_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), lo, P, host::bb_to_monty(g));
+    Status s = sync_after_build(ctx, stream, "bb_twist_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->lde_tabs.emplace(key, buf).first;
   }

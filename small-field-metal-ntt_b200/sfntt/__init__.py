@@ -142,6 +142,12 @@ class Context:
         """Bracket every later launch with CUDA events (clears old records)."""
         _check(self.handle, _ffi.lib().sfntt_kernel_timing(self.handle, int(enable)))
 
+    def butterfly_peak(self, gs: bool = True) -> float:
+        """Measured butterflies/s with register-resident data (integer ceiling)."""
+        out = ctypes.c_double()
+        _check(self.handle, _ffi.lib().sfntt_butterfly_peak(self.handle, int(gs), ctypes.byref(out)))
+        return out.value
+
     def kernel_times(self) -> dict:
         """{kernel: (launches, total_ms, algorithmic_bytes)} since kernel_timing()."""
         buf = ctypes.create_string_buffer(1 << 16)

@@ -46,6 +46,7 @@ SIGNATURES = {
     "sfntt_check_device_error": (i32, [vp]),
     "sfntt_kernel_timing": (i32, [vp, i32]),
     "sfntt_kernel_times": (i32, [vp, ctypes.c_char_p, sz]),
+    "sfntt_butterfly_peak": (i32, [vp, i32, ctypes.POINTER(ctypes.c_double)]),
 }
 
 _lib = None
