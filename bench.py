@@ -132,11 +132,13 @@ def peaks() -> tuple[float, str]:
 
 
 def ncu_traffic(kernel: str):
-    p = ROOT / "profiles" / "ncu_traffic.json"
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    p = ROOT / "profiles" / "ncu_traffic.txt"
     if p.exists():
-        d = json.loads(p.read_text())
-        if kernel in d:
-            return d[kernel]
+        for line in p.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#") and parts[0] == kernel:
+                return int(parts[1])
     return None
 
 

@@ -268,9 +268,10 @@ struct TPass {
   }
 
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
-    extern __shared__ uint8_t smem_raw[];
-    uint32_t* stage = reinterpret_cast<uint32_t*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
+    // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
+    // every access in the shared state space (LDS/STS, not generic LD/ST).
+    extern __shared__ __align__(1024) uint32_t smem_words[];
+    uint32_t* stage = smem_words;
     uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 2 * TWORDS);
     uint2* tws = reinterpret_cast<uint2*>(bar + 2);
     const uint32_t tid = threadIdx.x;
@@ -345,9 +346,10 @@ struct TExpand {
   static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
 
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
-    extern __shared__ uint8_t smem_raw[];
-    uint32_t* stage = reinterpret_cast<uint32_t*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~static_cast<uintptr_t>(1023u));
+    // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
+    // every access in the shared state space (LDS/STS, not generic LD/ST).
+    extern __shared__ __align__(1024) uint32_t smem_words[];
+    uint32_t* stage = smem_words;
     uint32_t* ostage = stage + 2 * TWORDS;
     uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 3 * TWORDS);
     uint2* tws_inv = reinterpret_cast<uint2*>(bar + 2);
