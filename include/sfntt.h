@@ -141,6 +141,21 @@ int sfntt_m31_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uin
 int sfntt_bb_to_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
 int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
 
+/* Allocation-free NTT (no counterpart in the reference).  For callers that
+ * cannot allocate device memory when they run a transform (a fixed memory
+ * pool, a locked-down allocator, a process that forbids device allocation
+ * after start-up): the out-of-place Stockham transform (variant V3), forward
+ * or inverse, in place on d_data, with its ping-pong partner in a file-scope
+ * device array of 2^20 words (4 MiB, held by every GPU that loads the
+ * library).  It calls no cudaMalloc/cudaFree.  Limits: batch << log_n <=
+ * 2^20 (else SFNTT_INVALID_SIZE); the twiddles for (field, log_n) must be
+ * resident (sfntt_prepare; else SFNTT_INVALID_ARGUMENT).  The first call on a
+ * device resolves the array's address (cudaGetSymbolAddress): make it before
+ * any stream capture.  All calls share the array; calls that overlap on the
+ * GPU race on it. */
+int sfntt_stockham_noalloc(sfntt_ctx *ctx, int field, int inverse, uint32_t *d_data, uint32_t log_n,
+                           uint32_t batch, void *stream);
+
 /* Pinned host memory for the host-buffer calls (full-bandwidth copies). */
 int sfntt_host_alloc(sfntt_ctx *ctx, size_t bytes, void **out);
 int sfntt_host_free(sfntt_ctx *ctx, void *p);

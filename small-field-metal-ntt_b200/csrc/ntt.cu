@@ -258,6 +258,16 @@ Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, 
   return layers_dev(ctx, field, inverse, in, out, in_stride, out_stride, log_n, batch, 0, log_n, scale, tw, s);
 }
 
+// One radix-2 layer between two device buffers, for entry points that
+// bring their own ping-pong partner (see noalloc.cu).
+Status stockham_layer_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out,
+                          const uint2* tw, uint32_t log_n, uint32_t L, uint32_t batch, uint32_t scale_w,
+                          cudaStream_t s) {
+  return layer(ctx, field, inverse, in, out, tw, log_n, L, batch, scale_w, s);
+}
+
+uint32_t inv_n_of(int field, uint32_t log_n) { return inv_n_canonical(field, log_n); }
+
 // Layers [a, b) of a forward / inverse network, in place; used by the M31
 // blow-up whose zero-padded top layers are a plain replication.
 Status ntt_layers_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint64_t stride, uint32_t log_n,

@@ -40,6 +40,7 @@ SIGNATURES = {
     "sfntt_m31_lde_dev": (i32, [vp, vp, vp, u32, u32, u32, vp]),
     "sfntt_bb_to_monty_dev": (i32, [vp, vp, sz, vp]),
     "sfntt_bb_from_monty_dev": (i32, [vp, vp, sz, vp]),
+    "sfntt_stockham_noalloc": (i32, [vp, i32, i32, vp, u32, u32, vp]),
     "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
     "sfntt_host_free": (i32, [vp, vp]),
     "sfntt_launch_count": (u64, [vp]),
