@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-secondary", action="store_true")
+    ap.add_argument("--workload", default="lde", choices=["lde", "uneven"],
+                    help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph")
+    ap.add_argument("--lanes", type=int, default=8)
     return ap.parse_args()
 
 
@@ -203,6 +206,9 @@ def main() -> None:
     if a.impl == "reference":
         run_reference(a, rank)
         return
+    if a.workload == "uneven":
+        run_uneven(a)
+        return
 
     import torch
     import torch.distributed as dist
@@ -335,6 +341,76 @@ def main() -> None:
             "roofline": roofline, "int_roofline": int_roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e,
             "cpu_baseline": cpu,
             "secondary": secondary, "device": ctx.device_info()}
+    print(json.dumps(line), flush=True)
+
+
+def run_uneven(a) -> None:
+    """The uneven-batch configuration: 64 polynomials, field 50/50 M31 /
+    BabyBear, log n uniform in 12..22, 1..128 columns, blow-up 1/2/4 with
+    probability 1/3 each, seeded; one plain launch sequence per polynomial vs
+    one autotuned CUDA-graph launch for the whole batch, outputs compared."""
+    import torch
+    import sfntt
+    torch.cuda.set_device(0)
+    ctx = sfntt.Context(0)
+    items = sfntt.uneven_workload(64, seed=2024)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(99)
+    keep = []
+    stream = torch.cuda.current_stream().cuda_stream
+    for it in items:
+        p = BB_P if it["field"] == sfntt.FIELD_BABYBEAR else 2147483647
+        x = torch.randint(0, p, (it["batch"] << it["log_n"],), dtype=torch.int64, device="cuda",
+                          generator=gen).to(torch.int32)
+        if it["field"] == sfntt.FIELD_BABYBEAR:
+            sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
+        y = torch.empty(it["batch"] << (it["log_n"] + it["added_bits"]), dtype=torch.int32, device="cuda")
+        it["d_in"], it["d_out"] = x.data_ptr(), y.data_ptr()
+        keep.append((x, y))
+    batch = sfntt.LdeBatch(ctx, items)
+    batch.prepare()
+    t0 = time.perf_counter()
+    batch.autotune(reps=1)
+    tune_s = time.perf_counter() - t0
+    plans = [batch.plan_of(i) for i in range(len(items))]
+
+    def timed(fn, steps):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def digest():
+        return [int(y.view(torch.int64 if y.numel() % 2 == 0 else torch.int32).sum().item()) for _, y in keep]
+
+    steps = max(3, min(a.steps, 20))
+    plain_ms = timed(lambda: batch.run(stream), steps)
+    d_plain = digest()
+    for _, y in keep:
+        y.zero_()
+    g = batch.graph(lanes=a.lanes)
+    graph_ms = timed(lambda: g.launch(stream), steps)
+    d_graph = digest()
+    elems_out = sum(it["batch"] << (it["log_n"] + it["added_bits"]) for it in items)
+    bytes_alg = sum(4 * (it["batch"] << it["log_n"]) * (1 + (1 << it["added_bits"])) for it in items)
+    peak, peak_kind = peaks()
+    line = {"metric": "uneven batch: 64 mixed M31/BabyBear LDEs", "unit": "ms", "value": graph_ms,
+            "plain_loop_ms": plain_ms, "graph_ms": graph_ms, "speedup": plain_ms / graph_ms,
+            "higher_is_better": False, "steps": steps, "warmup": a.warmup, "lanes": a.lanes,
+            "kernels_in_graph": g.kernel_count(), "outputs_identical": d_plain == d_graph,
+            "melem_per_s_out": elems_out / (graph_ms * 1e-3) / 1e6,
+            "hbm_frac": bytes_alg / (graph_ms * 1e-3) / (peak * 1e9), "autotune_s": tune_s,
+            "plans": {str(p): plans.count(p) for p in sorted(set(plans))},
+            "config": {"workload": "64 polynomials, field 50/50, log n U[12,22], columns U[1,128], "
+                                   "blow-up 1/2/4 (p = 1/3 each), seed 2024", "output_gb": bytes_alg / 1e9},
+            "data": "synthetic", "device": ctx.device_info()}
+    g.close()
     print(json.dumps(line), flush=True)
 
 

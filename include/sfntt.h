@@ -141,6 +141,49 @@ int sfntt_m31_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uin
 int sfntt_bb_to_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
 int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
 
+/* ---- Uneven batches in one graph launch (no reference counterpart: the
+ * north-star batching pattern).  An item is `batch` SoA columns of 2^log_n
+ * points of either field, extended by 2^added_bits: BabyBear items are the
+ * coset LDE of CosetLdeBatch::execute (src/lde/mod.rs:43-107, shift_monty 0 =
+ * reference shift), M31 items the composition inverse(odds(log_n)) -> zero-pad
+ * -> forward(odds(log_n + added_bits)).  Device pointers. */
+typedef enum sfntt_plan {
+    SFNTT_PLAN_AUTO = 0,           /* tuned plan for the item's key, else the context default */
+    SFNTT_PLAN_TMA = 1,            /* persistent TMA engine, per-position strided twiddles */
+    SFNTT_PLAN_TMA_FOUR_STEP = 2,  /* persistent TMA engine, four-step strided passes */
+    SFNTT_PLAN_TILE = 3            /* first (non-TMA) shared-memory tile engine */
+} sfntt_plan;
+
+typedef struct sfntt_lde_item {
+    int field;
+    uint32_t log_n, batch, added_bits, shift_monty;
+    const uint32_t *d_in;
+    uint32_t *d_out;
+    int plan;
+} sfntt_lde_item;
+
+typedef struct sfntt_graph sfntt_graph;
+
+/* Make every table the items need resident (required before capture). */
+int sfntt_batch_prepare(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count);
+/* The plain per-polynomial loop: one item after another on `stream`. */
+int sfntt_batch_run(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, void *stream);
+/* Capture all items into one CUDA graph; items are spread (largest first, to
+ * the least-loaded lane) over `lanes` forked streams so independent items
+ * overlap.  Replay with sfntt_graph_launch: one launch for the batch. */
+int sfntt_batch_graph_create(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int lanes,
+                             sfntt_graph **out);
+int sfntt_graph_launch(sfntt_graph *graph, void *stream);
+uint64_t sfntt_graph_kernel_count(const sfntt_graph *graph);
+void sfntt_graph_destroy(sfntt_graph *graph);
+/* Autotuner: for each distinct key (field, log_n, columns rounded up to a power
+ * of two, added_bits) time every plan `reps` times on the first item with that
+ * key and keep the fastest for SFNTT_PLAN_AUTO items.  The table is text. */
+int sfntt_autotune(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int reps);
+int sfntt_tune_save(sfntt_ctx *ctx, const char *path);
+int sfntt_tune_load(sfntt_ctx *ctx, const char *path);
+int sfntt_tune_lookup(sfntt_ctx *ctx, const sfntt_lde_item *item);
+
 /* Allocation-free NTT (no counterpart in the reference).  For callers that
  * cannot allocate device memory when they run a transform (a fixed memory
  * pool, a locked-down allocator, a process that forbids device allocation

@@ -114,6 +114,8 @@ struct sfntt_ctx {
   // for plain NTTs and the fused LDE.
   bool ntt_plain = SFNTT_NTT_PLAIN_DEFAULT;
   bool lde_plain = SFNTT_LDE_PLAIN_DEFAULT;
+  // autotuned plans: "field/log_n/columns/added_bits" -> sfntt_plan
+  std::map<std::string, int> tuned;
 
   // Opt-in per-kernel timing (sfntt_kernel_timing): an event pair around every
   // launch, resolved and aggregated by name in sfntt_kernel_times.

@@ -401,4 +401,90 @@ class M31Lde:
         _check(self.ctx.handle, st, batch_size << log_n)
 
 
+# ------------------------------------------------------- uneven batches ---
+PLAN_AUTO, PLAN_TMA, PLAN_TMA_FOUR_STEP, PLAN_TILE = 0, 1, 2, 3
+
+
+class LdeBatch:
+    """Uneven batch of LDE / blow-up items (both fields, device pointers) run
+    as a plain per-item loop, or captured once into a CUDA graph and replayed
+    with one launch (sfntt_batch_*, sfntt_graph_*).  Items are dicts with
+    keys field, log_n, batch, added_bits, d_in, d_out [, shift_monty, plan]."""
+
+    def __init__(self, ctx: Context, items: list[dict]):
+        self.ctx = ctx
+        arr = (_ffi.LdeItem * max(len(items), 1))()
+        for i, it in enumerate(items):
+            arr[i] = _ffi.LdeItem(it["field"], it["log_n"], it["batch"], it["added_bits"],
+                                  it.get("shift_monty", 0), it["d_in"], it["d_out"], it.get("plan", PLAN_AUTO))
+        self.items = arr
+        self.count = len(items)
+
+    def prepare(self) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_batch_prepare(self.ctx.handle, self.items, self.count))
+
+    def run(self, stream: int = 0) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_batch_run(self.ctx.handle, self.items, self.count, stream))
+
+    def autotune(self, reps: int = 2) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_autotune(self.ctx.handle, self.items, self.count, reps))
+
+    def plan_of(self, i: int) -> int:
+        return _ffi.lib().sfntt_tune_lookup(self.ctx.handle, ctypes.byref(self.items[i]))
+
+    def graph(self, lanes: int = 8) -> "Graph":
+        h = ctypes.c_void_p()
+        _check(self.ctx.handle, _ffi.lib().sfntt_batch_graph_create(self.ctx.handle, self.items, self.count, lanes,
+                                                                    ctypes.byref(h)))
+        return Graph(h)
+
+
+class Graph:
+    """An instantiated CUDA graph of a whole batch (sfntt_graph)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def launch(self, stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_graph_launch(self.handle, stream)
+        if st:
+            raise _ERRORS.get(st, NttError)(f"sfntt_graph_launch: status {st}")
+
+    def kernel_count(self) -> int:
+        return int(_ffi.lib().sfntt_graph_kernel_count(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            _ffi.lib().sfntt_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tune_save(ctx: Context, path: str) -> None:
+    _check(ctx.handle, _ffi.lib().sfntt_tune_save(ctx.handle, str(path).encode()))
+
+
+def tune_load(ctx: Context, path: str) -> None:
+    _check(ctx.handle, _ffi.lib().sfntt_tune_load(ctx.handle, str(path).encode()))
+
+
+def uneven_workload(n_items: int = 64, seed: int = 2024, log_n_range=(12, 22), cols_range=(1, 128),
+                    blowups=(0, 1, 2)) -> list[dict]:
+    """The uneven-batch configuration: field 50/50 M31 / BabyBear, log n and
+    columns uniform in their ranges, added_bits uniform over `blowups`
+    (blow-up 1/2/4), seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_items):
+        out.append({"field": int(rng.integers(0, 2)), "log_n": int(rng.integers(log_n_range[0], log_n_range[1] + 1)),
+                    "batch": int(rng.integers(cols_range[0], cols_range[1] + 1)),
+                    "added_bits": int(rng.choice(blowups))})
+    return out
+
+
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -41,6 +41,16 @@ SIGNATURES = {
     "sfntt_bb_to_monty_dev": (i32, [vp, vp, sz, vp]),
     "sfntt_bb_from_monty_dev": (i32, [vp, vp, sz, vp]),
     "sfntt_stockham_noalloc": (i32, [vp, i32, i32, vp, u32, u32, vp]),
+    "sfntt_batch_prepare": (i32, [vp, vp, sz]),
+    "sfntt_batch_run": (i32, [vp, vp, sz, vp]),
+    "sfntt_batch_graph_create": (i32, [vp, vp, sz, i32, ctypes.POINTER(vp)]),
+    "sfntt_graph_launch": (i32, [vp, vp]),
+    "sfntt_graph_kernel_count": (u64, [vp]),
+    "sfntt_graph_destroy": (None, [vp]),
+    "sfntt_autotune": (i32, [vp, vp, sz, i32]),
+    "sfntt_tune_save": (i32, [vp, ctypes.c_char_p]),
+    "sfntt_tune_load": (i32, [vp, ctypes.c_char_p]),
+    "sfntt_tune_lookup": (i32, [vp, vp]),
     "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
     "sfntt_host_free": (i32, [vp, vp]),
     "sfntt_launch_count": (u64, [vp]),
@@ -49,6 +59,13 @@ SIGNATURES = {
     "sfntt_kernel_times": (i32, [vp, ctypes.c_char_p, sz]),
     "sfntt_butterfly_peak": (i32, [vp, i32, ctypes.POINTER(ctypes.c_double)]),
 }
+
+class LdeItem(ctypes.Structure):
+    """sfntt_lde_item (include/sfntt.h)."""
+    _fields_ = [("field", ctypes.c_int), ("log_n", ctypes.c_uint32), ("batch", ctypes.c_uint32),
+                ("added_bits", ctypes.c_uint32), ("shift_monty", ctypes.c_uint32),
+                ("d_in", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("plan", ctypes.c_int)]
+
 
 _lib = None
 
