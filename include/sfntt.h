@@ -184,6 +184,48 @@ int sfntt_tune_save(sfntt_ctx *ctx, const char *path);
 int sfntt_tune_load(sfntt_ctx *ctx, const char *path);
 int sfntt_tune_lookup(sfntt_ctx *ctx, const sfntt_lde_item *item);
 
+/* Serving (no counterpart in the reference, whose API runs one request per
+ * call): a server admits LDE / blow-up requests of any size and either field
+ * as they arrive, with continuous batching.  It owns `slots` streams and one
+ * device arena of `budget_bytes` (the HBM admission budget, allocated once at
+ * creation).  Requests queue in submission order; sfntt_server_poll retires
+ * finished ones and admits queued ones, in order, while a slot is free and
+ * the arena has room for the request (its output; for host requests its
+ * input too), so requests that arrive while others run overlap with them on
+ * the device.  Tables stay resident in the context.  Results are exact, so a
+ * request gives the same output alone and in any mix.
+ *   sfntt_server_submit: input at item->d_in on the device (item->d_out is
+ *     ignored; the output lives in the arena until release).
+ *   sfntt_server_submit_host: input copied from h_in, output copied to h_out
+ *     (pinned memory for asynchronous copies) before the ticket completes.
+ * A request larger than the budget fails with SFNTT_ALLOC_FAILED.  BabyBear
+ * requests outside the fused LDE (log_n 0 or > 24, added_bits > 4) share the
+ * context's scratch and run alone.  A server is driven from one thread. */
+typedef struct sfntt_server sfntt_server;
+int sfntt_server_create(sfntt_ctx *ctx, size_t budget_bytes, int slots, sfntt_server **out);
+void sfntt_server_destroy(sfntt_server *server);
+int sfntt_server_submit(sfntt_server *server, const sfntt_lde_item *req, uint64_t *ticket);
+int sfntt_server_submit_host(sfntt_server *server, const sfntt_lde_item *req, const uint32_t *h_in,
+                             uint32_t *h_out, uint64_t *ticket);
+/* Retire finished requests, admit queued ones; writes up to `cap` finished
+ * tickets (oldest first; the rest are reported by later polls). */
+int sfntt_server_poll(sfntt_server *server, uint64_t *done, size_t cap, size_t *n_done);
+/* Device address of a finished request's output (valid until release). */
+int sfntt_server_result(sfntt_server *server, uint64_t ticket, uint32_t **d_out);
+/* Return a finished request's arena space. */
+int sfntt_server_release(sfntt_server *server, uint64_t ticket);
+/* Requests queued or running. */
+size_t sfntt_server_pending(const sfntt_server *server);
+/* Replay a request trace against the wall clock: request i is submitted
+ * arrival_s[i] seconds (sorted) after the start, finished requests are
+ * released at once; latency_s[i] = completion seen by the host - arrival.
+ * h_in / h_out: per-request host buffers (host requests), or both NULL
+ * (device inputs at reqs[i].d_in).  slots = 1 is the plain sequential
+ * per-request loop; slots > 1 batches continuously. */
+int sfntt_serve_trace(sfntt_ctx *ctx, const sfntt_lde_item *reqs, const uint32_t *const *h_in,
+                      uint32_t *const *h_out, const double *arrival_s, size_t count, int slots,
+                      size_t budget_bytes, double *latency_s, double *makespan_s);
+
 /* Allocation-free NTT (no counterpart in the reference).  For callers that
  * cannot allocate device memory when they run a transform (a fixed memory
  * pool, a locked-down allocator, a process that forbids device allocation

@@ -69,6 +69,8 @@ Status check_item(const sfntt_lde_item& it) {
   return {};
 }
 
+}  // namespace
+
 // Runs one item on stream s under its plan (tuned, explicit or default).
 Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
   SFNTT_TRY(check_item(it));
@@ -127,7 +129,6 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
   return {};
 }
 
-}  // namespace
 }  // namespace sfntt
 
 using sfntt::Status;

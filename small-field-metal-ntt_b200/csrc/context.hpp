@@ -160,6 +160,9 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
                   uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
                    uint32_t added_bits, cudaStream_t stream);
+// One LDE / blow-up work item (batch.cu): run under its plan, or make its tables resident.
+Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
+Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
 Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uint32_t* b, uint32_t* out,
                          size_t n, cudaStream_t stream);
 Status bb_monty_dev(sfntt_ctx* ctx, bool to_monty, uint32_t* d, size_t n, cudaStream_t stream);

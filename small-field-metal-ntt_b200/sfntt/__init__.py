@@ -487,4 +487,133 @@ def uneven_workload(n_items: int = 64, seed: int = 2024, log_n_range=(12, 22), c
     return out
 
 
+# ---------------------------------------------------------------- serving ---
+def _item_struct(it: dict) -> "_ffi.LdeItem":
+    return _ffi.LdeItem(it["field"], it["log_n"], it["batch"], it["added_bits"], it.get("shift_monty", 0),
+                        it.get("d_in", 0) or 0, 0, it.get("plan", PLAN_AUTO))
+
+
+class _DeviceWords:
+    """__cuda_array_interface__ view of n u32 words at a device address (as int32)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+class Server:
+    """Continuous-batching request server (sfntt_server_*): `slots` streams,
+    one device arena of `budget_bytes` (the HBM admission budget).  Requests
+    are dicts like LdeBatch items; `submit` takes the input at it["d_in"] on
+    the device, `submit_host` copies from / to host arrays.  `poll` retires
+    finished requests and admits queued ones in order while a slot is free
+    and the arena has room."""
+
+    def __init__(self, ctx: Context, budget_bytes: int, slots: int = 8):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        _check(ctx.handle, _ffi.lib().sfntt_server_create(ctx.handle, budget_bytes, slots, ctypes.byref(h)))
+        self.handle = h
+        self._host = {}  # ticket -> (in array, out array) kept alive until done
+
+    def submit(self, it: dict) -> int:
+        t = ctypes.c_uint64()
+        req = _item_struct(it)
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_submit(self.handle, ctypes.byref(req), ctypes.byref(t)))
+        return t.value
+
+    def submit_host(self, it: dict, x: np.ndarray) -> tuple[int, np.ndarray]:
+        """Returns (ticket, out); out is filled when the ticket completes."""
+        x = _u32(x)
+        out = np.empty(it["batch"] << (it["log_n"] + it["added_bits"]), dtype=np.uint32)
+        t = ctypes.c_uint64()
+        req = _item_struct(it)
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_submit_host(
+            self.handle, ctypes.byref(req), x.ctypes.data, out.ctypes.data, ctypes.byref(t)))
+        self._host[t.value] = (x, out)
+        return t.value, out
+
+    def poll(self, cap: int = 256) -> list[int]:
+        buf = (ctypes.c_uint64 * cap)()
+        n = ctypes.c_size_t()
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_poll(self.handle, buf, cap, ctypes.byref(n)))
+        done = [int(buf[i]) for i in range(n.value)]
+        for t in done:
+            self._host.pop(t, None)
+        return done
+
+    def result_ptr(self, ticket: int) -> int:
+        p = ctypes.c_void_p()
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_result(self.handle, ticket, ctypes.byref(p)))
+        return p.value
+
+    def result(self, ticket: int, n_words: int):
+        """A torch int32 view of a finished request's output (valid until release)."""
+        import torch
+        return torch.as_tensor(_DeviceWords(self.result_ptr(ticket), n_words), device=f"cuda:{self.ctx.device}")
+
+    def release(self, ticket: int) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_release(self.handle, ticket))
+
+    def pending(self) -> int:
+        return int(_ffi.lib().sfntt_server_pending(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            _ffi.lib().sfntt_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_trace(ctx: Context, reqs: list[dict], arrivals, slots: int, budget_bytes: int,
+                host: list[tuple[np.ndarray, np.ndarray]] | None = None) -> tuple[np.ndarray, float]:
+    """Replays a trace (sfntt_serve_trace): request i submitted at arrivals[i]
+    seconds; returns (latency seconds per request, makespan seconds).  slots=1
+    is the plain sequential per-request loop.  `host`: per-request (input,
+    output) host arrays for host requests, else inputs at d_in on the device."""
+    n = len(reqs)
+    arr = (_ffi.LdeItem * max(n, 1))()
+    for i, it in enumerate(reqs):
+        arr[i] = _item_struct(it)
+    t_arr = np.ascontiguousarray(arrivals, dtype=np.float64)
+    lat = np.zeros(n, dtype=np.float64)
+    mk = ctypes.c_double()
+    dbl = ctypes.POINTER(ctypes.c_double)
+    h_in = h_out = None
+    if host is not None:
+        h_in = (ctypes.c_void_p * max(n, 1))(*[h[0].ctypes.data for h in host])
+        h_out = (ctypes.c_void_p * max(n, 1))(*[h[1].ctypes.data for h in host])
+    _check(ctx.handle, _ffi.lib().sfntt_serve_trace(ctx.handle, arr, h_in, h_out, t_arr.ctypes.data_as(dbl), n, slots,
+                                                    budget_bytes, lat.ctypes.data_as(dbl), ctypes.byref(mk)))
+    return lat, mk.value
+
+
+SERVED_LOG_N_WEIGHTS = {14: 1, 15: 1, 16: 2, 17: 3, 18: 6, 19: 6, 20: 6, 21: 2, 22: 1}
+
+
+def served_workload(n_requests: int, rate: float, seed: int = 2025, cols_range=(8, 256), blowups=(1, 2),
+                    log_n_weights: dict | None = None) -> tuple[list[dict], np.ndarray]:
+    """The served stream: Poisson arrivals at `rate` req/s; field 50/50 M31 /
+    BabyBear; log n in 14..22 weighted toward 18-20; columns uniform in
+    cols_range; blow-up 2 or 4 (added_bits 1 or 2); seeded.  Returns
+    (requests without buffers, sorted arrival times in seconds)."""
+    w = log_n_weights or SERVED_LOG_N_WEIGHTS
+    rng = np.random.default_rng(seed)
+    logs = np.array(sorted(w), dtype=np.int64)
+    p = np.array([w[k] for k in logs], dtype=np.float64)
+    p /= p.sum()
+    reqs = []
+    for _ in range(n_requests):
+        reqs.append({"field": int(rng.integers(0, 2)), "log_n": int(rng.choice(logs, p=p)),
+                     "batch": int(rng.integers(cols_range[0], cols_range[1] + 1)),
+                     "added_bits": int(rng.choice(blowups))})
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    return reqs, arrivals
+
+
 __all__ = [n for n in dir() if not n.startswith("_")]

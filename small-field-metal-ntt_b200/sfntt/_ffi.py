@@ -51,6 +51,16 @@ SIGNATURES = {
     "sfntt_tune_save": (i32, [vp, ctypes.c_char_p]),
     "sfntt_tune_load": (i32, [vp, ctypes.c_char_p]),
     "sfntt_tune_lookup": (i32, [vp, vp]),
+    "sfntt_server_create": (i32, [vp, sz, i32, ctypes.POINTER(vp)]),
+    "sfntt_server_destroy": (None, [vp]),
+    "sfntt_server_submit": (i32, [vp, vp, u64p]),
+    "sfntt_server_submit_host": (i32, [vp, vp, vp, vp, u64p]),
+    "sfntt_server_poll": (i32, [vp, u64p, sz, ctypes.POINTER(sz)]),
+    "sfntt_server_result": (i32, [vp, u64, ctypes.POINTER(vp)]),
+    "sfntt_server_release": (i32, [vp, u64]),
+    "sfntt_server_pending": (sz, [vp]),
+    "sfntt_serve_trace": (i32, [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_double), sz, i32, sz,
+                                ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
     "sfntt_host_free": (i32, [vp, vp]),
     "sfntt_launch_count": (u64, [vp]),
