@@ -28,6 +28,12 @@ constexpr uint32_t kTileWords = 1u << kTileBits;
 constexpr uint32_t kTileBytes = 4u << kTileBits;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: far beyond any tile's latency
 
+// Contiguous tiles are moved with the 128-byte TMA swizzle: word c of the tile
+// sits at c ^ (((c >> 5) & 7) << 2) in shared memory.  Without it, rounds whose
+// threads own tile bits 0..3 (four consecutive words, 128-bit accesses) hit
+// 4-way bank conflicts; with it every round but one is conflict-free.
+constexpr bool kSwizzleC = true;
+
 struct TmaArgs {
   const uint2* tw;     // twiddles (layer-concatenated Shoup pairs)
   uint32_t log_n;      // positions per column of this network
@@ -181,33 +187,58 @@ struct TPass {
     return mp.mpos[0] == 0 && mp.mpos[1] == 1;
   }
 
+  // Shared-memory word of tile word c (the TMA layout of this tile kind).
+  static constexpr bool kSwz = (KD == Kind::C) && kSwizzleC;
+  __host__ __device__ static constexpr uint32_t sw(uint32_t c) { return kSwz ? c ^ (((c >> 5) & 7u) << 2) : c; }
+  // Bits that sw(x) may set when x ranges over the bits of `mask`.
+  __host__ __device__ static constexpr uint32_t sw_support(uint32_t mask) { return sw(mask) | mask; }
+  // sw is linear over GF(2), so sw(ct | cm) = sw(ct) ^ sw(cm).  Round k's
+  // thread part and slot part overlap only in the bits `overlap<k>()`; the
+  // rest of sw(cm) is added as an immediate offset:
+  //   sw(ct | cm) = (sw(ct) ^ (sw(cm) & O)) + (sw(cm) & ~O).
+  template <int k>
+  __device__ static constexpr uint32_t overlap() {
+    constexpr RoundMap mp = make_map<KD, P, LT, R>(k);
+    uint32_t tmask = 0, cmask = 0;
+    for (int g = 0; g < mp.ngrp; ++g) tmask |= mp.gmask[g] << mp.gshift[g];
+    for (int j = 0; j < R; ++j) cmask |= 1u << mp.mpos[j];
+    return sw_support(tmask) & sw_support(cmask);
+  }
+  template <int k>
+  __device__ static __forceinline__ uint32_t addr(uint32_t sct, int m) {
+    using M = RM<KD, P, LT, R, k>;
+    constexpr uint32_t O = overlap<k>();
+    const uint32_t scm = sw(M::cm(m));
+    return (sct ^ (scm & O)) + (scm & ~O);
+  }
+
   template <int k>
   __device__ static __forceinline__ void ld(const uint32_t* st, uint32_t (&v)[E], uint32_t tid) {
     using M = RM<KD, P, LT, R, k>;
-    const uint32_t* p = st + M::ctid(tid);
+    const uint32_t sct = sw(M::ctid(tid));
     if constexpr (vec<k>()) {
 #pragma unroll
       for (int m = 0; m < E; m += 4) {
-        const uint4 q = *reinterpret_cast<const uint4*>(p + M::cm(m));
+        const uint4 q = *reinterpret_cast<const uint4*>(st + addr<k>(sct, m));
         v[m] = q.x; v[m + 1] = q.y; v[m + 2] = q.z; v[m + 3] = q.w;
       }
     } else {
 #pragma unroll
-      for (int m = 0; m < E; ++m) v[m] = p[M::cm(m)];
+      for (int m = 0; m < E; ++m) v[m] = st[addr<k>(sct, m)];
     }
   }
 
   template <int k>
   __device__ static __forceinline__ void st(uint32_t* st, const uint32_t (&v)[E], uint32_t tid) {
     using M = RM<KD, P, LT, R, k>;
-    uint32_t* p = st + M::ctid(tid);
+    const uint32_t sct = sw(M::ctid(tid));
     if constexpr (vec<k>()) {
 #pragma unroll
       for (int m = 0; m < E; m += 4)
-        *reinterpret_cast<uint4*>(p + M::cm(m)) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+        *reinterpret_cast<uint4*>(st + addr<k>(sct, m)) = make_uint4(v[m], v[m + 1], v[m + 2], v[m + 3]);
     } else {
 #pragma unroll
-      for (int m = 0; m < E; ++m) p[M::cm(m)] = v[m];
+      for (int m = 0; m < E; ++m) st[addr<k>(sct, m)] = v[m];
     }
   }
 

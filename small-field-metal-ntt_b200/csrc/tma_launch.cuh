@@ -27,8 +27,10 @@ struct TmaRequest {
 };
 
 // Resolved once through the runtime (no link-time dependency on libcuda).
+// swizzle128: 128-byte swizzle of the box in shared memory (16-byte chunk j of
+// 128-byte row r lands at chunk j ^ (r & 7); the buffer is 1024-byte aligned).
 Status tensor_map_encode(CUtensorMap* map, const void* base, uint32_t rank, const cuuint64_t* dims,
-                         const cuuint64_t* strides_bytes, const cuuint32_t* box);
+                         const cuuint64_t* strides_bytes, const cuuint32_t* box, bool swizzle128 = false);
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
@@ -56,7 +58,7 @@ inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n,
     dims[0] = 32; dims[1] = (uint64_t)batch * n / 32; dims[2] = 1;
     strides[0] = 128; strides[1] = (uint64_t)batch * n * 4;
   }
-  return tensor_map_encode(m, base, 3, dims, strides, box);
+  return tensor_map_encode(m, base, 3, dims, strides, box, kSwizzleC);
 }
 
 // column viewed as [hb][e][lchunk][u]: u 32 words, lchunk 2^lo/32, e 2^P (stride 2^lo), hb
