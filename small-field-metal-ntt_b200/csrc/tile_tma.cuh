@@ -369,6 +369,7 @@ tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__
 // inverse layers [lo, log_n), then for each output block q the multiplier
 // M_q[pos] (n^-1, coset shift, zero-padded top layers) and forward layers
 // [lo, log_n); block q goes to rows [q n, (q+1) n) of the extended column.
+// The inverse result stays in registers across the blocks.
 template <int P, bool PLAIN>
 struct TExpand {
   using Inv = TPass<BabyBear, false, Kind::S, P, PLAIN>;
@@ -407,6 +408,7 @@ struct TExpand {
     }
     using M = RM<Kind::S, P, LT, R, K - 1>;
     const uint32_t ct = M::ctid(tid);
+    const uint32_t lo = ai.lo;
     const uint32_t n = 1u << ai.log_n;
     const uint32_t nq = 1u << ai.log_q;
     uint32_t x[E], v[E];
@@ -432,17 +434,20 @@ struct TExpand {
       Inv::template ld<0>(cur, x, tid);
       Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout, values in [0, 2p)
       // position of slot m: pos_base + u + (e << lo)
-      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << ai.lo);
+      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
       for (uint32_t q = 0; q < nq; ++q) {
         uint32_t* ob = (q & 1u) ? ostage : cur;
-        if (q >= 2) {  // ob was last used by block q-2's store
+        // The TMA store that last read ob is the one before the newest pending
+        // store (for q = 1: the previous tile's last ostage store, which no
+        // prefetch wait covers on a CTA's last tile).
+        if (q >= 1) {
           if (tid == 0) tma::wait_reads_1();
           __syncthreads();
         }
         const uint2* mq = ai.mul + (uint64_t)q * n + pos_t;
 #pragma unroll
         for (int m = 0; m < E; ++m) {
-          const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << ai.lo));
+          const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
           v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
         }
         Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, g, tid);  // forward starts in round K-1's layout
