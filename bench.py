@@ -329,6 +329,7 @@ def main() -> None:
         hout.free()
 
     secondary = None if a.no_secondary else secondary_metrics(ctx, sfntt, torch)
+    layouts = None if a.no_secondary else layout_metrics(a, ctx, sfntt, torch, x, out, stream)
     del x, out
     torch.cuda.empty_cache()
     served = None if (a.no_served or world > 1) else served_sweep(a, ctx, sfntt, torch)
@@ -351,8 +352,49 @@ def main() -> None:
             "melem_per_s_out": a.batch * n_ext / (value * 1e-3) / 1e6,
             "roofline": roofline, "int_roofline": int_roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e,
             "cpu_baseline": cpu,
-            "secondary": secondary, "served": served, "device": ctx.device_info()}
+            "secondary": secondary, "layout": layouts, "served": served, "device": ctx.device_info()}
     print(json.dumps(line), flush=True)
+
+
+def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
+    """The callers either side of the LDE: natural row order (Plonky3's
+    coset_lde_batch convention) and the row-major Merkle-commitment layout of
+    the LDE output (HBM-bound permutations: every word read and written once),
+    plus the whole LDE in the natural-order convention."""
+    n_ext = 1 << (a.log_n + a.added_bits)
+    total = a.batch * n_ext
+    peak, _ = peaks()
+    rows = torch.empty_like(out)
+
+    def timed(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    res = {"workload": f"LDE output, {a.batch} columns x 2^{a.log_n + a.added_bits} rows ({4 * total / 2**30:.0f} GiB)"}
+    lb = a.log_n + a.added_bits
+    for name, fn in (("natural_in_place", lambda: sfntt.layout_dev(ctx, out.data_ptr(), out.data_ptr(), lb, a.batch,
+                                                                   sfntt.LAYOUT_NATURAL, stream)),
+                     ("row_major", lambda: sfntt.layout_dev(ctx, out.data_ptr(), rows.data_ptr(), lb, a.batch,
+                                                            sfntt.LAYOUT_ROW_MAJOR, stream)),
+                     ("row_major_natural", lambda: sfntt.layout_dev(ctx, out.data_ptr(), rows.data_ptr(), lb, a.batch,
+                                                                    sfntt.LAYOUT_ROW_MAJOR | sfntt.LAYOUT_NATURAL,
+                                                                    stream))):
+        ms = timed(fn)
+        gbs = 8 * total / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "gbs": gbs, "hbm_frac": gbs / peak}
+    lde_nat = sfntt.CosetLdeBatch(ctx, natural=True)
+    ms = timed(lambda: lde_nat.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream))
+    res["lde_natural_order_ms"] = ms
+    del rows
+    return res
 
 
 def served_sweep(a, ctx, sfntt, torch) -> dict:

@@ -62,7 +62,9 @@ typedef enum sfntt_variant {
 /* Coset-LDE forms (src/lde/mod.rs:43-107). */
 typedef enum sfntt_lde_mode {
     SFNTT_LDE_FUSED = 0,   /* normalize+shift+zero-pad folded into the adjacent NTT passes */
-    SFNTT_LDE_UNFUSED = 1  /* iDFT -> normalize -> zero-pad -> shift -> DFT, one kernel each */
+    SFNTT_LDE_UNFUSED = 1, /* iDFT -> normalize -> zero-pad -> shift -> DFT, one kernel each */
+    SFNTT_LDE_NATURAL = 2  /* flag, OR'ed into either form: natural-order output rows (Plonky3's
+                              convention, with shift_monty = to_monty(31)); no reference counterpart */
 } sfntt_lde_mode;
 
 typedef struct sfntt_ctx sfntt_ctx;
@@ -136,6 +138,26 @@ int sfntt_bb_coset_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out
                            void *stream);
 int sfntt_m31_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
                       uint32_t batch, uint32_t added_bits, void *stream);
+
+/* ---- Output conventions of SoA batches (either field; no reference
+ * counterpart beyond its one-word-per-thread bitrev_permute kernel,
+ * shaders/m31/m31_ntt_ct_dit_r2.metal:22-41).  Flags:
+ *   SFNTT_LAYOUT_NATURAL    rows of every column from bit-reversed to natural
+ *                           order: out[c*n + r] = in[c*n + bitrev(r)]
+ *   SFNTT_LAYOUT_ROW_MAJOR  transpose to row-major rows (Merkle-commitment
+ *                           input, one leaf per row): out[R*batch + c] = in[c*n + r],
+ *                           R = bitrev(r) with SFNTT_LAYOUT_NATURAL, else r
+ * n = 2^log_n.  d_in == d_out is allowed for SFNTT_LAYOUT_NATURAL alone (in
+ * place, no scratch); otherwise the buffers must not overlap. */
+typedef enum sfntt_layout_flags {
+    SFNTT_LAYOUT_NATURAL = 1,
+    SFNTT_LAYOUT_ROW_MAJOR = 2
+} sfntt_layout_flags;
+int sfntt_layout_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n, uint32_t batch,
+                     int flags, void *stream);
+/* Host buffers (len must equal batch << log_n); *gpu_ns = device time. */
+int sfntt_layout(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n, uint32_t batch, int flags,
+                 uint32_t *out, uint64_t *gpu_ns);
 
 /* BabyBear::to_monty / from_monty (src/field/babybear.rs:54-65) on device. */
 int sfntt_bb_to_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);

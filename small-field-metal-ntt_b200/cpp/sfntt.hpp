@@ -254,10 +254,13 @@ struct LdeResult {
 
 // CosetLdeBatch (src/lde/mod.rs:15-107): iDFT -> x n^-1 -> zero-pad ->
 // x shift^i -> DFT over batch_size BabyBear columns.
+// natural = true: natural-order input evaluations and output rows (Plonky3's
+// coset_lde_batch convention) instead of the reference's bit-reversed ones.
 class CosetLdeBatch {
  public:
-  explicit CosetLdeBatch(Context ctx = Context(), bool fused = true)
-      : ctx_(std::move(ctx)), mode_(fused ? SFNTT_LDE_FUSED : SFNTT_LDE_UNFUSED) {}
+  explicit CosetLdeBatch(Context ctx = Context(), bool fused = true, bool natural = false)
+      : ctx_(std::move(ctx)),
+        mode_((fused ? SFNTT_LDE_FUSED : SFNTT_LDE_UNFUSED) | (natural ? SFNTT_LDE_NATURAL : 0)) {}
   static CosetLdeBatch create(const std::string& /*shader_dir*/ = {}, int device = 0) {
     return CosetLdeBatch(Context(device));
   }
@@ -310,6 +313,24 @@ class M31Lde {
  private:
   Context ctx_;
 };
+
+// ---- output layout ------------------------------------------------------------
+// Row order / row-major form of a SoA batch: SFNTT_LAYOUT_NATURAL (bit-reversed
+// rows -> natural), SFNTT_LAYOUT_ROW_MAJOR (out[row * batch + col], the
+// Merkle-commitment input).  Returns (out, device ns).
+inline std::pair<std::vector<uint32_t>, uint64_t> layout(const Context& ctx, std::span<const uint32_t> in,
+                                                         uint32_t log_n, uint32_t batch, int flags) {
+  std::vector<uint32_t> out(in.size());
+  uint64_t ns = 0;
+  detail::check(ctx.handle(), sfntt_layout(ctx.handle(), in.data(), in.size(), log_n, batch, flags, out.data(), &ns),
+                in.size());
+  return {std::move(out), ns};
+}
+inline void layout_dev(const Context& ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                       int flags, void* stream = nullptr) {
+  detail::check(ctx.handle(), sfntt_layout_dev(ctx.handle(), d_in, d_out, log_n, batch, flags, stream),
+                (size_t)batch << log_n);
+}
 
 // ---- uneven batches in one graph launch -----------------------------------
 enum class Plan : int { Auto = SFNTT_PLAN_AUTO, Tma = SFNTT_PLAN_TMA, TmaFourStep = SFNTT_PLAN_TMA_FOUR_STEP,

@@ -216,7 +216,7 @@ int api_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, uint32_t 
   if (field == SFNTT_M31 && log_ext > 30) s = {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (s.ok() && len != ((size_t)batch << log_n))  // src/lde/mod.rs:54-56
     s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != batch << log_n"};
-  if (s.ok() && mode != SFNTT_LDE_FUSED && mode != SFNTT_LDE_UNFUSED) s = {SFNTT_INVALID_ARGUMENT, "unknown mode"};
+  if (s.ok() && (mode & ~(SFNTT_LDE_UNFUSED | SFNTT_LDE_NATURAL))) s = {SFNTT_INVALID_ARGUMENT, "unknown mode"};
   if (s.ok() && len && (!in || !out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
   if (s.ok() && len) s = run_host_lde(ctx, field, in, out, log_n, batch, added_bits, shift_monty, mode, ns);
   return finish(ctx, s);
@@ -450,6 +450,43 @@ int sfntt_m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uin
   Status s;
   if (batch && (!d_in || !d_out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
   if (s.ok()) s = sfntt::m31_lde_dev(ctx, d_in, d_out, log_n, batch, added_bits, (cudaStream_t)stream);
+  return finish(ctx, s);
+}
+
+int sfntt_layout_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch, int flags,
+                     void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::layout_dev(ctx, d_in, d_out, log_n, batch, flags, (cudaStream_t)stream));
+}
+
+int sfntt_layout(sfntt_ctx* ctx, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch, int flags,
+                 uint32_t* out, uint64_t* ns) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  if (ns) *ns = 0;
+  Status s;
+  if (log_n >= 40 || len != ((size_t)batch << log_n))
+    s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != batch << log_n"};
+  if (s.ok() && len && (!in || !out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  if (s.ok() && len) {
+    s = [&]() -> Status {
+      const size_t bytes = len * sizeof(uint32_t);
+      SFNTT_TRY(ctx->buf_in.reserve(bytes));
+      SFNTT_TRY(ctx->buf_out.reserve(bytes));
+      uint32_t* din = ctx->buf_in.as<uint32_t>();
+      uint32_t* dout = ctx->buf_out.as<uint32_t>();
+      SFNTT_CU(cudaMemcpyAsync(din, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_start, ctx->stream));
+      SFNTT_TRY(sfntt::layout_dev(ctx, din, dout, log_n, batch, flags, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_stop, ctx->stream));
+      SFNTT_CU(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      SFNTT_CU(cudaStreamSynchronize(ctx->stream));
+      return elapsed_ns(ctx, ns);
+    }();
+  }
   return finish(ctx, s);
 }
 

@@ -205,9 +205,12 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
 
 }  // namespace
 
-Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
-                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
-  if (mode != SFNTT_LDE_FUSED && mode != SFNTT_LDE_UNFUSED) return {SFNTT_INVALID_ARGUMENT, "unknown LDE mode"};
+namespace {
+
+// Input columns at stride in_stride (n, or n_ext when they already sit in the
+// output columns); output bit-reversed rows.
+Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uint32_t* d_out, uint32_t log_n,
+                   uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
   const uint32_t log_ext = log_n + added_bits;
   if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
   if (batch == 0) return {};
@@ -233,8 +236,8 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
         SFNTT_TRY(bb_twist_table(ctx, lo, 8, false, s, &tw_f));
       }
       const uint32_t mask = (uint32_t)(n - 1);
-      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s,
-                           tw_i, mask));
+      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, in_stride, n_ext, log_n, batch, 0, lo, 0u, tw_inv,
+                           s, tw_i, mask));
       if (plain)
         SFNTT_TRY((launch_tma_expand<8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s)));
       else
@@ -248,7 +251,7 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
     if (lo > 0) {  // I1: inverse layers [0, lo) into the output buffer
       PassRequest r{};
       r.args.in = d_in; r.args.out = d_out; r.args.tw = tw_inv;
-      r.args.in_stride = n; r.args.out_stride = n_ext;
+      r.args.in_stride = in_stride; r.args.out_stride = n_ext;
       r.args.log_n = log_n; r.args.lo = 0; r.P = (int)lo; r.contiguous = true; r.batch = batch;
       SFNTT_TRY(run_pass_bb_inv(ctx, r, s));
     }
@@ -256,7 +259,7 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
     ea.inv.in = lo > 0 ? d_out : d_in;
     ea.inv.out = d_out;
     ea.inv.tw = tw_inv;
-    ea.inv.in_stride = lo > 0 ? n_ext : n;
+    ea.inv.in_stride = lo > 0 ? n_ext : in_stride;
     ea.inv.out_stride = n_ext;
     ea.inv.log_n = log_n;
     ea.inv.lo = lo;
@@ -279,10 +282,10 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
   SFNTT_TRY(ctx->buf_aux.reserve(bytes));
   uint32_t* coeffs = ctx->buf_aux.as<uint32_t>();
   if (log_n > 0) {
-    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_BABYBEAR, true, d_in, coeffs, n, n, log_n, batch, false, s));
+    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_BABYBEAR, true, d_in, coeffs, in_stride, n, log_n, batch, false, s));
     SFNTT_TRY(scale_dev(ctx, SFNTT_BABYBEAR, coeffs, n * batch, host::invmod((uint32_t)n, host::BB_P), s));
   } else {
-    SFNTT_CU(cudaMemcpyAsync(coeffs, d_in, bytes, cudaMemcpyDeviceToDevice, s));
+    SFNTT_CU(cudaMemcpy2DAsync(coeffs, 4, d_in, in_stride * 4, 4, batch, cudaMemcpyDeviceToDevice, s));
   }
   SFNTT_TRY(zero_pad_dev(ctx, coeffs, d_out, log_n, batch, added_bits, s));
   const uint2* shift_tab = nullptr;
@@ -290,6 +293,28 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
   SFNTT_TRY(mul_table_dev(ctx, d_out, log_ext, batch, shift_tab, s));
   if (log_ext > 0) SFNTT_TRY(ntt_dev(ctx, SFNTT_BABYBEAR, SFNTT_V4_CT_GS_R4, false, d_out, log_ext, batch, s));
   return {};
+}
+
+}  // namespace
+
+// The reference's convention: input evaluations and output rows in
+// bit-reversed order.  SFNTT_LDE_NATURAL (Plonky3's coset_lde_batch):
+// natural-order input and output; the input columns are bit-reversed into the
+// output columns, the LDE runs there in place, and the output columns are
+// bit-reversed in place.
+Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+  if (mode & ~(SFNTT_LDE_UNFUSED | SFNTT_LDE_NATURAL)) return {SFNTT_INVALID_ARGUMENT, "unknown LDE mode"};
+  const int form = mode & SFNTT_LDE_UNFUSED;
+  if (!(mode & SFNTT_LDE_NATURAL))
+    return bb_lde_rows(ctx, d_in, 1ull << log_n, d_out, log_n, batch, added_bits, shift_monty, form, s);
+  const uint32_t log_ext = log_n + added_bits;
+  if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
+  if (batch == 0) return {};
+  const uint64_t n_ext = 1ull << log_ext;
+  SFNTT_TRY(bitrev_cols_dev(ctx, d_in, 1ull << log_n, d_out, n_ext, log_n, batch, s));
+  SFNTT_TRY(bb_lde_rows(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, shift_monty, form, s));
+  return bitrev_cols_dev(ctx, d_out, n_ext, d_out, n_ext, log_ext, batch, s);
 }
 
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,

@@ -30,6 +30,8 @@ FIELD_M31 = 0
 FIELD_BABYBEAR = 1
 BEST, V1, V2, V3, V4 = 0, 1, 2, 3, 4
 LDE_FUSED, LDE_UNFUSED = 0, 1
+LDE_NATURAL = 2  # flag: natural-order input and output rows (Plonky3's coset_lde_batch)
+LAYOUT_NATURAL, LAYOUT_ROW_MAJOR = 1, 2
 
 
 # --------------------------------------------------------------- errors ---
@@ -349,9 +351,11 @@ class LdeResult:
 class CosetLdeBatch:
     """CosetLdeBatch (src/lde/mod.rs:15-107)."""
 
-    def __init__(self, ctx: Context | None = None, device: int = 0, fused: bool = True):
+    def __init__(self, ctx: Context | None = None, device: int = 0, fused: bool = True, natural: bool = False):
+        """natural=True: natural-order input evaluations and output rows
+        (Plonky3's convention) instead of the reference's bit-reversed ones."""
         self.ctx = ctx or default_context(device)
-        self.mode = LDE_FUSED if fused else LDE_UNFUSED
+        self.mode = (LDE_FUSED if fused else LDE_UNFUSED) | (LDE_NATURAL if natural else 0)
 
     @classmethod
     def new(cls, shader_dir=None, device: int = 0):
@@ -399,6 +403,26 @@ class M31Lde:
                     stream: int = 0) -> None:
         st = _ffi.lib().sfntt_m31_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits, stream)
         _check(self.ctx.handle, st, batch_size << log_n)
+
+
+# -------------------------------------------------------- output layout ---
+def layout(data, log_n: int, batch: int, flags: int, ctx: Context | None = None) -> tuple[np.ndarray, int]:
+    """Row order / row-major form of a SoA batch (sfntt_layout): flags
+    LAYOUT_NATURAL (bit-reversed rows -> natural), LAYOUT_ROW_MAJOR
+    (out[row * batch + col], the Merkle-commitment input).  -> (out, device ns)."""
+    ctx = ctx or default_context()
+    inp = _u32(data)
+    out = np.empty_like(inp)
+    ns = ctypes.c_uint64()
+    st = _ffi.lib().sfntt_layout(ctx.handle, _p(inp), inp.size, log_n, batch, flags, _p(out), ctypes.byref(ns))
+    _check(ctx.handle, st, inp.size)
+    return out, int(ns.value)
+
+
+def layout_dev(ctx: Context, in_ptr: int, out_ptr: int, log_n: int, batch: int, flags: int, stream: int = 0) -> None:
+    """Device pointers; in place (in_ptr == out_ptr) for LAYOUT_NATURAL alone."""
+    st = _ffi.lib().sfntt_layout_dev(ctx.handle, in_ptr, out_ptr, log_n, batch, flags, stream)
+    _check(ctx.handle, st, batch << log_n)
 
 
 # ------------------------------------------------------- uneven batches ---

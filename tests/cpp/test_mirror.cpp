@@ -159,6 +159,38 @@ void check_lde(const sfntt::Context& ctx) {
   CHECK(invalid, "CosetLdeBatch InvalidSize(input.len())");
 }
 
+std::vector<uint32_t> bitrev_cols(const std::vector<uint32_t>& x, uint32_t log_n, uint32_t batch) {
+  std::vector<uint32_t> y(x.size());
+  const size_t n = size_t(1) << log_n;
+  for (size_t c = 0; c < batch; ++c)
+    for (size_t r = 0; r < n; ++r) {
+      size_t rr = 0;
+      for (uint32_t b = 0; b < log_n; ++b) rr |= ((r >> b) & 1) << (log_n - 1 - b);
+      y[c * n + rr] = x[c * n + r];
+    }
+  return y;
+}
+
+void check_layout(const sfntt::Context& ctx) {
+  const uint32_t log_n = 11, batch = 5;
+  const size_t n = size_t(1) << log_n;
+  auto x = lcg(size_t(batch) << log_n, 61, false);
+  auto [nat, ns] = sfntt::layout(ctx, x, log_n, batch, SFNTT_LAYOUT_NATURAL);
+  CHECK(nat == bitrev_cols(x, log_n, batch), "layout natural");
+  auto [rows, ns2] = sfntt::layout(ctx, x, log_n, batch, SFNTT_LAYOUT_ROW_MAJOR);
+  bool ok = true;
+  for (size_t c = 0; c < batch; ++c)
+    for (size_t r = 0; r < n; ++r) ok &= rows[r * batch + c] == x[c * n + r];
+  CHECK(ok, "layout row-major");
+  // Plonky3 convention: natural-order input and output rows
+  const uint32_t lb = 12, cols = 3, added = 1;
+  auto xn = lcg(size_t(cols) << lb, 62, true);
+  std::vector<uint32_t> ref(size_t(cols) << (lb + added));
+  orc_bb_coset_lde(bitrev_cols(xn, lb, cols).data(), ref.data(), lb, cols, added, orc_bb_to_monty(31), 4);
+  auto r = sfntt::CosetLdeBatch(ctx, true, true).execute(xn, lb, cols, added, orc_bb_to_monty(31));
+  CHECK(r.data == bitrev_cols(ref, lb + added, cols), "CosetLdeBatch natural (Plonky3 convention)");
+}
+
 void check_server(const sfntt::Context& ctx) {
   // host requests of both fields and uneven sizes, admitted as slots and
   // arena space free up; each must equal the oracle (= the request alone)
@@ -226,6 +258,7 @@ int main(int argc, char** argv) {
     check_backend<sfntt::BabyBear, sfntt::Variant::CtGsR4>(ctx);
     check_pointwise_and_batch(ctx);
     check_lde(ctx);
+    check_layout(ctx);
     check_server(ctx);
   }
   std::printf("%d checks, %d failed\n", g_checks, g_fail);
