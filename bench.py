@@ -393,6 +393,11 @@ def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
     lde_nat = sfntt.CosetLdeBatch(ctx, natural=True)
     ms = timed(lambda: lde_nat.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream))
     res["lde_natural_order_ms"] = ms
+    # the M31 blow-up of the same shape (inputs < BabyBear p are canonical M31 values)
+    m31 = sfntt.M31Lde(ctx)
+    ctx.prepare_lde(sfntt.FIELD_M31, a.log_n, a.added_bits)
+    res["m31_lde_ms"] = timed(lambda: m31.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits,
+                                                      stream=stream))
     del rows
     return res
 

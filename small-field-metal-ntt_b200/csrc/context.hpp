@@ -160,6 +160,8 @@ Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_
                   uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
                    uint32_t added_bits, cudaStream_t stream);
+// n^-1 mod p, canonical (ntt.cu).
+uint32_t inv_n_of(int field, uint32_t log_n);
 // Row-order / row-major permutations of SoA batches (layout.cu); bitrev_cols_dev
 // permutes each column's rows with separate column strides (in place if in == out).
 Status bitrev_cols_dev(sfntt_ctx* ctx, const uint32_t* in, uint64_t in_stride, uint32_t* out, uint64_t out_stride,

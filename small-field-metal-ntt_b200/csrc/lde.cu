@@ -173,11 +173,12 @@ __global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, 
   }
 }
 
-template <int P, bool PLAIN>
+// mul: BabyBear multiplier table M_q; scale_w: M31's n^-1 (canonical).
+template <class F, int P, bool PLAIN>
 Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_stride, uint32_t* d_out, uint32_t log_n,
                          uint32_t batch, uint32_t added_bits, const uint2* tw_inv, const uint2* tw_fwd,
-                         const uint2* mul, cudaStream_t s) {
-  using X = TExpand<P, PLAIN>;
+                         const uint2* mul, cudaStream_t s, uint32_t scale_w = 0) {
+  using X = TExpand<F, P, PLAIN>;
   const uint32_t lo = log_n - P;
   const uint64_t n = 1ull << log_n, n_ext = n << added_bits;
   CUtensorMap min, mout;
@@ -193,13 +194,16 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   a.log_q = added_bits;
   a.err = ctx->err.as<int>();
   a.ntiles = (uint32_t)(((uint64_t)batch * n) >> (P + 5));
+  a.scale_w = scale_w;
+  a.scale_ws = (uint32_t)(((uint64_t)scale_w << 32) / F::P);
   constexpr int smem = 3 * (int)X::TBYTES + 16 + 16 * (int)X::Inv::TW_ENTRIES + 1024;
-  auto kern = tma_expand_kernel<P, PLAIN>;
+  auto kern = tma_expand_kernel<F, P, PLAIN>;
   SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, X::NT, smem, s>>>(min, mout, a);
-  static const std::string name = "bb_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "");
+  static const std::string name =
+      std::string(F::kMontgomery ? "bb" : "m31") + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "");
   return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
 }
 
@@ -239,9 +243,11 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
       SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, in_stride, n_ext, log_n, batch, 0, lo, 0u, tw_inv,
                            s, tw_i, mask));
       if (plain)
-        SFNTT_TRY((launch_tma_expand<8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s)));
+        SFNTT_TRY((launch_tma_expand<BabyBear, 8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
+                                                        tw_fwd, mul, s)));
       else
-        SFNTT_TRY((launch_tma_expand<8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd, mul, s)));
+        SFNTT_TRY((launch_tma_expand<BabyBear, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
+                                                         tw_fwd, mul, s)));
       SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd,
                            s, tw_f, mask));
       return {};
@@ -323,6 +329,19 @@ Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32
   if (log_ext > 30) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (batch == 0) return {};
   const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
+  if (!ctx->no_tma && log_n >= 13 && added_bits <= 4 && aligned16(d_in) && aligned16(d_out)) {
+    // I1: inverse layers [0, lo) into the output columns; X: inverse layers
+    // [lo, log_n), n^-1, and per output block forward layers [lo, log_n) of
+    // the extended network; F3: forward layers [0, lo) of the extended network.
+    const uint32_t lo = log_n - 8;
+    const uint2 *tw_inv = nullptr, *tw_fwd = nullptr;
+    SFNTT_TRY(m31_twiddles(ctx, true, log_n, s, &tw_inv));
+    SFNTT_TRY(m31_twiddles(ctx, false, log_ext, s, &tw_fwd));
+    SFNTT_TRY(layers_dev(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s));
+    SFNTT_TRY((launch_tma_expand<M31, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd,
+                                                nullptr, s, inv_n_of(SFNTT_M31, log_n))));
+    return layers_dev(ctx, SFNTT_M31, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd, s);
+  }
   if (log_n > 0) {
     SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, true, s));
   } else {

@@ -39,7 +39,6 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocMaxWords];
 Status stockham_layer_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out,
                           const uint2* tw, uint32_t log_n, uint32_t L, uint32_t batch, uint32_t scale_w,
                           cudaStream_t s);
-uint32_t inv_n_of(int field, uint32_t log_n);
 
 namespace {
 

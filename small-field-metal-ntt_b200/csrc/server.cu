@@ -4,15 +4,19 @@
 // (allocated once, at creation; requests never call cudaMalloc).  Requests are
 // queued in arrival order; sfntt_server_poll retires finished requests
 // (event query, arena space returned) and admits queued ones, in order, while
-// a slot is free and the arena has room for the request's output.  Admitted
-// requests run on their slot's stream, so work of requests that arrive while
-// others are on the GPU overlaps on the device.  Twiddle and multiplier tables
-// stay resident in the context across requests.
+// a slot is free, the arena has room for the request, and the GPU has room:
+// a request's width is the fraction of the GPU its widest pass fills
+// (min(1, tiles / (2 * SMs)), 2^13-word tiles), and requests run together only
+// while their widths add up to at most one.  A request that fills the GPU by
+// itself therefore runs alone, as in the plain loop; small requests that
+// arrive while others run are packed beside them and overlap on the device.
+// Twiddle and multiplier tables stay resident in the context across requests.
 //
 // sfntt_serve_trace replays a request trace against the wall clock: request i
 // is submitted at arrival_s[i] after the start; with slots = 1 the server is
 // the plain sequential per-request loop (one request in flight, the next one
 // admitted when it finishes), with slots > 1 it batches continuously.
+#include <algorithm>
 #include <chrono>
 #include <deque>
 #include <map>
@@ -68,6 +72,7 @@ class Arena {
 
 struct Request {
   uint64_t ticket;
+  double width = 1.0;  // fraction of the GPU the request fills
   sfntt_lde_item item;
   const uint32_t* h_in = nullptr;  // host request: input copied into the arena
   uint32_t* h_out = nullptr;       // host request: result copied back here
@@ -94,6 +99,7 @@ struct sfntt_server {
   std::map<uint64_t, Request> running, finished;
   std::deque<uint64_t> ready;  // finished, not yet reported by poll
   bool exclusive_running = false;
+  double occupancy = 0;  // sum of the running requests' widths
   uint64_t next_ticket = 1;
 };
 
@@ -120,6 +126,7 @@ Status admit(sfntt_server* sv) {
     if (slot < 0) return {};
     Request& r = sv->queue.front();
     if (!sv->running.empty() && (exclusive(r.item) || sv->exclusive_running)) return {};
+    if (!sv->running.empty() && sv->occupancy + r.width > 1.0 + 1e-9) return {};  // the GPU is full
     size_t off = 0;
     if (!sv->arena->alloc(arena_bytes(r), &off)) return {};  // in order: wait for memory
     r.off = off;
@@ -145,6 +152,7 @@ Status admit(sfntt_server* sv) {
     }
     sv->slot_req[slot] = (int64_t)r.ticket;
     sv->exclusive_running = exclusive(r.item);
+    sv->occupancy += r.width;
     r.item.d_out = it.d_out;
     sv->running.emplace(r.ticket, r);
     sv->queue.pop_front();
@@ -161,9 +169,13 @@ Status retire(sfntt_server* sv) {
     const uint64_t t = (uint64_t)sv->slot_req[s];
     sv->slot_req[s] = -1;
     auto it = sv->running.find(t);
+    sv->occupancy = std::max(0.0, sv->occupancy - it->second.width);
     sv->finished.emplace(t, it->second);
     sv->running.erase(it);
-    if (sv->running.empty()) sv->exclusive_running = false;
+    if (sv->running.empty()) {
+      sv->exclusive_running = false;
+      sv->occupancy = 0;
+    }
     sv->ready.push_back(t);
   }
   return {};
@@ -253,6 +265,8 @@ int submit(sfntt_server* sv, const sfntt_lde_item* req, const uint32_t* h_in, ui
   r.item.d_out = nullptr;
   if (r.item.batch && !h_in && !r.item.d_in) return SFNTT_INVALID_ARGUMENT;
   if (r.item.log_n + r.item.added_bits > 30) return finish(sv->ctx, {SFNTT_INVALID_SIZE, "log_n + added_bits > 30"});
+  const double tiles = (double)((uint64_t)r.item.batch << (r.item.log_n + r.item.added_bits)) / 8192.0;
+  r.width = std::min(1.0, tiles / (2.0 * sv->ctx->sm_count));
   if (arena_bytes(r) > sv->budget)
     return finish(sv->ctx, {SFNTT_ALLOC_FAILED, "request exceeds the server's HBM budget"});
   int prev = -1;

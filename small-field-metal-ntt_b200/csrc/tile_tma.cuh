@@ -55,9 +55,13 @@ struct TmaArgs {
   uint32_t log_q;
 };
 
-// The forward half of the LDE expansion reads the forward twiddle table.
+// The forward half of the LDE expansion runs in the extended network: the
+// forward twiddle table, 2^(log_n + log_q) positions.
 struct FwdArgs : TmaArgs {
-  __device__ explicit FwdArgs(const TmaArgs& a) : TmaArgs(a) { tw = a.tw_fwd; }
+  __device__ explicit FwdArgs(const TmaArgs& a) : TmaArgs(a) {
+    tw = a.tw_fwd;
+    log_n = a.log_n + a.log_q;
+  }
 };
 __device__ __forceinline__ FwdArgs fwd_args(const TmaArgs& a) { return FwdArgs(a); }
 
@@ -365,17 +369,23 @@ tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
-// Fused coset-LDE middle step on Kind::S tiles (P <= 8, lo = log_n - P):
-// inverse layers [lo, log_n), then for each output block q the multiplier
-// M_q[pos] (n^-1, coset shift, zero-padded top layers) and forward layers
-// [lo, log_n); block q goes to rows [q n, (q+1) n) of the extended column.
+// Fused LDE middle step on Kind::S tiles (P <= 8, lo = log_n - P): inverse
+// layers [lo, log_n), then for each output block q forward layers [lo, log_n)
+// of the extended network (the block's tiles sit in high block q of it);
+// block q goes to rows [q n, (q+1) n) of the extended column.
+//   BabyBear: before block q's forward layers, the multiplier M_q[pos] (n^-1,
+//     coset shift, zero-padded top layers).
+//   M31: the inverse result times n^-1 once; the zero-padded top forward layers
+//     are a plain replication (CT butterfly on (a, 0) gives (a, a)), so every
+//     block starts from the same values.
 // The inverse result stays in registers across the blocks.
-template <int P, bool PLAIN>
+template <class F, int P, bool PLAIN>
 struct TExpand {
-  using Inv = TPass<BabyBear, false, Kind::S, P, PLAIN>;
-  using Fwd = TPass<BabyBear, true, Kind::S, P, PLAIN>;
+  using Inv = TPass<F, false, Kind::S, P, PLAIN>;
+  using Fwd = TPass<F, true, Kind::S, P, PLAIN>;
   static constexpr int K = Inv::K, E = Inv::E, NT = Inv::NT, R = Inv::R, LT = Inv::LT;
   static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
+  static_assert(F::kMontgomery || !PLAIN, "M31 passes have no plain variant");
 
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
@@ -432,7 +442,11 @@ struct TExpand {
       }
       const typename Inv::Geo g = Inv::geo(ai, t);
       Inv::template ld<0>(cur, x, tid);
-      Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout, values in [0, 2p)
+      Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
+      if constexpr (!F::kMontgomery) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) x[m] = mul_shoup<F>(x[m], ai.scale_w, ai.scale_ws);  // n^-1
+      }
       // position of slot m: pos_base + u + (e << lo)
       const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
       for (uint32_t q = 0; q < nq; ++q) {
@@ -444,13 +458,24 @@ struct TExpand {
           if (tid == 0) tma::wait_reads_1();
           __syncthreads();
         }
-        const uint2* mq = ai.mul + (uint64_t)q * n + pos_t;
+        if constexpr (F::kMontgomery) {
+          const uint2* mq = ai.mul + (uint64_t)q * n + pos_t;
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-          const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
-          v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
+          for (int m = 0; m < E; ++m) {
+            const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
+            v[m] = mul_shoup<F>(x[m], w.x, w.y);
+          }
+        } else {
+#pragma unroll
+          for (int m = 0; m < E; ++m) v[m] = x[m];
         }
-        Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, g, tid);  // forward starts in round K-1's layout
+        typename Inv::Geo gq = g;
+        gq.hb = q;  // high block of the extended network (M31 per-block twiddles)
+        Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, gq, tid);  // forward starts in round K-1's layout
+        if constexpr (!Net<F, true>::kGS) {
+#pragma unroll
+          for (int m = 0; m < E; ++m) v[m] = reduce2p<F>(v[m]);  // lazy CT values to [0, p)
+        }
         Fwd::template st<0>(ob, v, tid);
         tma::fence_proxy_async();
         __syncthreads();
@@ -464,10 +489,10 @@ struct TExpand {
   }
 };
 
-template <int P, bool PLAIN>
-__global__ void __launch_bounds__(TExpand<P, PLAIN>::NT, 1)
+template <class F, int P, bool PLAIN>
+__global__ void __launch_bounds__(TExpand<F, P, PLAIN>::NT, 1)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
-  TExpand<P, PLAIN>::run(&min, &mout, a);
+  TExpand<F, P, PLAIN>::run(&min, &mout, a);
 }
 
 }  // namespace sfntt

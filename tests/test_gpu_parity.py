@@ -263,6 +263,24 @@ def test_m31_lde_matches_composition(ctx, golden):
     for case in meta["m31_lde"]:
         r = m.execute(arr[case["input"]], case["log_n"], case["batch"], case["added_bits"])
         assert np.array_equal(r.data, arr[case["output"]])
-    for (ln, b, ab) in ((12, 3, 1), (14, 2, 2), (16, 2, 1)):
+    # log_n >= 13 runs the fused TMA path (inverse, n^-1, replication, forward in one kernel)
+    for (ln, b, ab) in ((12, 3, 1), (13, 2, 1), (14, 2, 2), (16, 2, 1), (17, 1, 3), (15, 3, 4), (20, 2, 1)):
         x = O.lcg(b << ln, ln, O.M31_P)
-        assert np.array_equal(m.execute(x, ln, b, ab).data, O.m31_lde(x, ln, b, ab, threads=4)), (ln, b, ab)
+        assert np.array_equal(m.execute(x, ln, b, ab).data, O.m31_lde(x, ln, b, ab, threads=8)), (ln, b, ab)
+
+
+def test_m31_lde_full_size_sampled_columns(ctx):
+    """2^20 x 128 M31 blow-up: sampled columns against the oracle; the
+    inverse of the extension is the input followed by zeros on every column."""
+    log_n, batch, added = 20, 128, 1
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    x = O.lcg(batch << log_n, 77, O.M31_P)
+    r = sfntt.M31Lde(ctx).execute(x, log_n, batch, added)
+    for c in (0, batch // 2 + 1, batch - 1):
+        assert np.array_equal(r.data[c * n_ext:(c + 1) * n_ext], O.m31_lde(x[c * n:(c + 1) * n], log_n, 1, added)), c
+    m31 = sfntt.CudaCtGsR4(ctx)
+    ext, _ = m31.inverse_ntt_batch_gpu(r.data, log_n + added, batch)
+    base, _ = m31.inverse_ntt_batch_gpu(x, log_n, batch)
+    ext = ext.reshape(batch, n_ext)
+    assert not ext[:, n:].any()
+    assert np.array_equal(ext[:, :n], base.reshape(batch, n))
