@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--added-bits", type=int, default=1)
     ap.add_argument("--mode", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--shift", default="31", choices=["31", "reference"],
+                    help="coset shift: g = 31 (the multiplicative generator) or the reference's default "
+                         "two_adic_generator(log_n_ext + 1); the cost is the same")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -63,10 +66,18 @@ def parse():
     return ap.parse_args()
 
 
+def shift_monty(a) -> int:
+    """Montgomery form of the coset shift (0 = the reference default)."""
+    if a.shift == "reference":
+        return 0
+    return (31 << 32) % BB_P  # to_monty(31) = 31 * 2^32 mod p
+
+
 def workload(a) -> dict:
     return {"workload": f"BabyBear coset LDE 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x blow-up",
             "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
-            "shift": "two_adic_generator(log_n_ext+1) (reference default)",
+            "shift": "g = 31, row i times 31^i" if a.shift == "31" else
+                     "two_adic_generator(log_n_ext+1) (reference default)",
             "layout": "SoA column-major, Montgomery u32",
             "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
                   f"{4 * a.batch << (a.log_n + a.added_bits) >> 20} MiB out per step)"}
@@ -159,13 +170,13 @@ def cpu_lde_sample(a, target_s: float) -> dict:
     n = 1 << a.log_n
     one = O.lcg(n, 1, BB_P, monty=True)
     t = time.perf_counter()
-    O.bb_coset_lde(one, a.log_n, 1, a.added_bits, threads=1)
+    O.bb_coset_lde(one, a.log_n, 1, a.added_bits, shift_monty=shift_monty(a), threads=1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(target_s * threads / max(t1, 1e-6)))))
     cols = max(1, min(a.batch, (cols // threads) * threads or cols))
     x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
     t = time.perf_counter()
-    O.bb_coset_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+    O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a), threads=threads)
     ts = time.perf_counter() - t
     return {"value": ts * 1e3 * a.batch / cols, "unit": "ms", "cores": threads, "kind": "port",
             "sample": f"{cols} of {a.batch} columns (oracle/oracle.c coset_lde, OpenMP over columns), "
@@ -181,14 +192,14 @@ def run_reference(a, rank: int) -> None:
     n = 1 << a.log_n
     per_step = max(0.3, min(20.0, 150.0 / max(1, a.steps + a.warmup)))  # whole run ~2.5 min
     t = time.perf_counter()
-    O.bb_coset_lde(O.lcg(n, 1, BB_P, monty=True), a.log_n, 1, a.added_bits, threads=1)
+    O.bb_coset_lde(O.lcg(n, 1, BB_P, monty=True), a.log_n, 1, a.added_bits, shift_monty=shift_monty(a), threads=1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(per_step * threads / max(t1, 1e-6)))))
     x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
     times = []
     for i in range(a.warmup + a.steps):
         t = time.perf_counter()
-        O.bb_coset_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+        O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a), threads=threads)
         if i >= a.warmup:
             times.append((time.perf_counter() - t) * a.batch / cols)
     ms = statistics.mean(times) * 1e3
@@ -211,33 +222,20 @@ def main() -> None:
     if a.impl == "reference":
         run_reference(a, rank)
         return
-    if a.workload == "uneven":
-        run_uneven(a)
-        return
-    if a.workload == "served":
-        run_served(a)
+    if a.workload in ("uneven", "served"):
+        if rank == 0:  # single-GPU workloads: under torchrun the other ranks have no work
+            (run_uneven if a.workload == "uneven" else run_served)(a)
         return
 
     import torch
-    import torch.distributed as dist
     import sfntt
+    from sfntt.replicas import Replicas, job_time_per_unit
 
     torch.cuda.set_device(local)
-    dist_on = world > 1
-    if dist_on:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist_on:
-            dist.barrier()
-
-    def max_all(v: float) -> float:
-        if not dist_on:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    # N GPUs = N independent replicas; the process group only carries the
+    # barrier and the max of per-rank times (no data-path collective)
+    rep = Replicas(backend="nccl", timeout_s=120, device=torch.device("cuda", local))
+    barrier, max_all = rep.barrier, rep.max
 
     ctx = sfntt.Context(local)
     lde = sfntt.CosetLdeBatch(ctx, fused=(a.mode == "fused"))
@@ -248,10 +246,11 @@ def main() -> None:
     out = torch.empty(a.batch * n_ext, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
-    ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, 0)
+    shift = shift_monty(a)
+    ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, shift)
 
     def step():
-        lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream)
+        lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, shift_monty=shift, stream=stream)
 
     for _ in range(a.warmup):
         step()
@@ -278,7 +277,7 @@ def main() -> None:
     ctx.kernel_timing(False)
     clocks = sampler.stop(w0, w1)
     step_ms = max_all(ev0.elapsed_time(ev1) / a.steps)
-    value = step_ms / world
+    value = job_time_per_unit(step_ms, world)
 
     # dominant kernel and its roofline
     peak, peak_kind = peaks()
@@ -312,12 +311,12 @@ def main() -> None:
         hin = ctx.pinned(a.batch * n)
         hout = ctx.pinned(a.batch * n_ext)
         hin.array[:] = x.cpu().numpy().view("uint32")
-        lde.execute(hin.array, a.log_n, a.batch, a.added_bits, out=hout.array)  # warm-up
+        lde.execute(hin.array, a.log_n, a.batch, a.added_bits, shift_monty=shift, out=hout.array)  # warm-up
         barrier()
         ts = []
         for _ in range(a.e2e_steps):
             t = time.perf_counter()
-            lde.execute(hin.array, a.log_n, a.batch, a.added_bits, out=hout.array)
+            lde.execute(hin.array, a.log_n, a.batch, a.added_bits, shift_monty=shift, out=hout.array)
             ts.append(time.perf_counter() - t)
         e2e_ms = max_all(statistics.mean(ts) * 1e3)
         ok = bool((hout.array[: n_ext] == out[: n_ext].cpu().numpy().view("uint32")).all())
@@ -338,8 +337,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_lde_sample(a, a.cpu_seconds)
 
-    if dist_on:
-        dist.destroy_process_group()
+    rep.close()
     if rank != 0:
         return
     line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
@@ -556,13 +554,19 @@ def kernel_butterflies(name: str, bytes_per_launch: int, added_bits: int) -> flo
 
 
 def secondary_metrics(ctx, sfntt, torch) -> dict:
-    """The other two parts of the headline metric string: single-column NTT
-    throughput (Gelem/s) and the M31 2^16 forward+inverse pair."""
-    res = {}
+    """The single-column NTT configurations: BabyBear forward + inverse for
+    log n = 10..24 and the M31 Circle NTT likewise (n = 2^16 is the M31
+    configuration), values uniform in [0, p), device-resident, 50 timed pairs
+    after 5 warm-up pairs.  Columns up to 2^24 words (64 MiB) stay resident in
+    the 126 MB L2 across repetitions, so the byte fraction is against HBM
+    bandwidth for reference only.  Gelem/s counts n per transform."""
+    res = {"note": "forward+inverse pairs on one device-resident column (L2-resident up to 2^24)"}
     stream = torch.cuda.current_stream().cuda_stream
-    for field, name, sizes in ((sfntt.FIELD_BABYBEAR, "bb", (16, 20, 24)), (sfntt.FIELD_M31, "m31", (16, 20))):
+    peak, _ = peaks()
+    for field, name in ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31")):
         b = (sfntt.BbCudaCtGsR4 if field == sfntt.FIELD_BABYBEAR else sfntt.CudaCtGsR4)(ctx)
-        for log_n in sizes:
+        rows = {}
+        for log_n in range(10, 25):
             p = BB_P if field == sfntt.FIELD_BABYBEAR else 2147483647
             d = torch.randint(0, p, (1 << log_n,), dtype=torch.int64, device="cuda").to(torch.int32)
             ctx.prepare(field, log_n)
@@ -578,8 +582,13 @@ def secondary_metrics(ctx, sfntt, torch) -> dict:
             e1.record()
             torch.cuda.synchronize()
             us = e0.elapsed_time(e1) * 1e3 / reps
-            res[f"{name}_fwd_inv_2^{log_n}_us"] = us
-            res[f"{name}_ntt_2^{log_n}_gelem_s"] = 2 * (1 << log_n) / (us * 1e-6) / 1e9
+            n = 1 << log_n
+            rows[str(log_n)] = {"fwd_inv_us": us, "gelem_s": 2 * n / (us * 1e-6) / 1e9,
+                                "gbs": 16 * n / (us * 1e-6) / 1e9, "hbm_frac": 16 * n / (us * 1e-6) / 1e9 / peak}
+        res[name] = rows
+        best = max(rows.items(), key=lambda kv: kv[1]["gelem_s"])
+        res[f"{name}_best_gelem_s"] = {"log_n": int(best[0]), "gelem_s": best[1]["gelem_s"]}
+    res["m31_2^16_fwd_inv_us"] = res["m31"]["16"]["fwd_inv_us"]
     return res
 
 
