@@ -272,6 +272,13 @@ int sfntt_host_free(sfntt_ctx *ctx, void *p);
  * SFNTT_TIMEOUT; after _dev calls, synchronise the stream and call this. */
 int sfntt_check_device_error(sfntt_ctx *ctx);
 
+/* Self-test of the bounded device-side wait (no reference counterpart): runs
+ * the tile engine's mbarrier wait on a barrier that nothing arrives on
+ * (arrive = 0; returns SFNTT_TIMEOUT after timeout_ns, clamped to 1 us..1 s)
+ * or that gets its arrival (arrive = 1; returns SFNTT_OK).  The context stays
+ * usable either way. */
+int sfntt_selftest_bounded_wait(sfntt_ctx *ctx, uint64_t timeout_ns, int arrive);
+
 /* Number of kernels this library has launched through ctx (for launch counts). */
 uint64_t sfntt_launch_count(const sfntt_ctx *ctx);
 

@@ -160,6 +160,12 @@ class Context:
             out[name] = (int(launches), float(ms), int(nbytes))
         return out
 
+    def selftest_bounded_wait(self, timeout_ns: int, arrive: bool) -> int:
+        """Runs the tile engine's bounded mbarrier wait on a barrier that
+        nothing arrives on (arrive=False) or that gets its arrival; returns
+        the status (SFNTT_TIMEOUT = 8 or 0) without raising."""
+        return int(_ffi.lib().sfntt_selftest_bounded_wait(self.handle, timeout_ns, int(arrive)))
+
     def prepare(self, field: int, log_n: int) -> None:
         _check(self.handle, _ffi.lib().sfntt_prepare(self.handle, field, log_n))
 

@@ -40,6 +40,7 @@ SIGNATURES = {
     "sfntt_m31_lde_dev": (i32, [vp, vp, vp, u32, u32, u32, vp]),
     "sfntt_bb_to_monty_dev": (i32, [vp, vp, sz, vp]),
     "sfntt_layout_dev": (i32, [vp, vp, vp, u32, u32, i32, vp]),
+    "sfntt_selftest_bounded_wait": (i32, [vp, u64, i32]),
     "sfntt_layout": (i32, [vp, u32p, sz, u32, u32, i32, u32p, u64p]),
     "sfntt_bb_from_monty_dev": (i32, [vp, vp, sz, vp]),
     "sfntt_stockham_noalloc": (i32, [vp, i32, i32, vp, u32, u32, vp]),
