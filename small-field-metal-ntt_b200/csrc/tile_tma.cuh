@@ -173,13 +173,44 @@ struct TPass {
     constexpr int r = Plan<P, R>::r(k);
     constexpr int b = Plan<P, R>::b(k);
     const uint32_t ct = M::ctid(tid);
+    if constexpr (!F::kMontgomery && KD == Kind::C && r == R) {
+      // M31 contiguous round without filler bits: slot m sits at tile bits
+      // m << b, so layer L = b + j needs tw[L][(pos_base + ct) >> (L+1) + o]
+      // for o = m >> (j+1) < 2^(r-1-j): consecutive entries from an even
+      // index (n - n/2^L, pos_base >> (L+1) and the thread's bits above the
+      // round are even multiples there), fetched as 128-bit pairs.
 #pragma unroll
-    for (int jj = 0; jj < r; ++jj) {
-      const int j = DESC ? (r - 1 - jj) : jj;
+      for (int jj = 0; jj < r; ++jj) {
+        const int j = DESC ? (r - 1 - jj) : jj;
+        const uint32_t L = (uint32_t)(b + j);
+        const uint32_t n = 1u << a.log_n;
+        const uint2* base = a.tw + (n - (n >> L)) + (g.pos_base >> (L + 1)) + (ct >> (L + 1));
+        uint2 tv[E / 2];
+        if (j == r - 1) {
+          tv[0] = __ldg(base);
+        } else {
 #pragma unroll
-      for (int m = 0; m < E; ++m) {
-        if (m & (1 << j)) continue;
-        butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, tws, g, ct, m, b + j));
+          for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(base + o));
+            tv[o] = make_uint2(q.x, q.y);
+            tv[o + 1] = make_uint2(q.z, q.w);
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          if (m & (1 << j)) continue;
+          butterfly<F, DESC>(v[m], v[m | (1 << j)], tv[m >> (j + 1)]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int jj = 0; jj < r; ++jj) {
+        const int j = DESC ? (r - 1 - jj) : jj;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          if (m & (1 << j)) continue;
+          butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, tws, g, ct, m, b + j));
+        }
       }
     }
   }
