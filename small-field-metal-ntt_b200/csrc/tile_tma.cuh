@@ -173,18 +173,21 @@ struct TPass {
     constexpr int r = Plan<P, R>::r(k);
     constexpr int b = Plan<P, R>::b(k);
     const uint32_t ct = M::ctid(tid);
-    if constexpr (!F::kMontgomery && KD == Kind::C && r == R) {
-      // M31 contiguous round without filler bits: slot m sits at tile bits
-      // m << b, so layer L = b + j needs tw[L][(pos_base + ct) >> (L+1) + o]
-      // for o = m >> (j+1) < 2^(r-1-j): consecutive entries from an even
-      // index (n - n/2^L, pos_base >> (L+1) and the thread's bits above the
+    if constexpr (!F::kMontgomery && r == R) {
+      // M31 round without filler bits: slot m sits at group bits m << b, so
+      // layer L = lo + b + j needs the per-block twiddles tw[L][base + o] for
+      // o = m >> (j+1) < 2^(r-1-j): consecutive entries from an even index
+      // (n - n/2^L, the tile's block offset and the thread's bits above the
       // round are even multiples there), fetched as 128-bit pairs.
 #pragma unroll
       for (int jj = 0; jj < r; ++jj) {
         const int j = DESC ? (r - 1 - jj) : jj;
-        const uint32_t L = (uint32_t)(b + j);
+        const uint32_t beta = (uint32_t)(b + j);
+        const uint32_t L = a.lo + beta;
         const uint32_t n = 1u << a.log_n;
-        const uint2* base = a.tw + (n - (n >> L)) + (g.pos_base >> (L + 1)) + (ct >> (L + 1));
+        const uint2* base = a.tw + (n - (n >> L));
+        if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + (ct >> (L + 1));
+        else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
         uint2 tv[E / 2];
         if (j == r - 1) {
           tv[0] = __ldg(base);
