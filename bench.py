@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--slots", type=int, default=8, help="served stream: concurrent request slots")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="served stream: HBM admission budget")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served"],
+    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table"],
                     help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph")
     ap.add_argument("--lanes", type=int, default=8)
     return ap.parse_args()
@@ -222,9 +222,9 @@ def main() -> None:
     if a.impl == "reference":
         run_reference(a, rank)
         return
-    if a.workload in ("uneven", "served"):
+    if a.workload in ("uneven", "served", "table"):
         if rank == 0:  # single-GPU workloads: under torchrun the other ranks have no work
-            (run_uneven if a.workload == "uneven" else run_served)(a)
+            {"uneven": run_uneven, "served": run_served, "table": run_table}[a.workload](a)
         return
 
     import torch
@@ -471,14 +471,17 @@ def run_served(a) -> None:
 
 
 def run_uneven(a) -> None:
+    import torch
+    import sfntt
+    torch.cuda.set_device(0)
+    print(json.dumps(uneven_metrics(a, sfntt.Context(0), sfntt, torch)), flush=True)
+
+
+def uneven_metrics(a, ctx, sfntt, torch) -> dict:
     """The uneven-batch configuration: 64 polynomials, field 50/50 M31 /
     BabyBear, log n uniform in 12..22, 1..128 columns, blow-up 1/2/4 with
     probability 1/3 each, seeded; one plain launch sequence per polynomial vs
     one autotuned CUDA-graph launch for the whole batch, outputs compared."""
-    import torch
-    import sfntt
-    torch.cuda.set_device(0)
-    ctx = sfntt.Context(0)
     items = sfntt.uneven_workload(64, seed=2024)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(99)
@@ -537,7 +540,120 @@ def run_uneven(a) -> None:
                                    "blow-up 1/2/4 (p = 1/3 each), seed 2024", "output_gb": bytes_alg / 1e9},
             "data": "synthetic", "device": ctx.device_info()}
     g.close()
-    print(json.dumps(line), flush=True)
+    del keep
+    torch.cuda.empty_cache()
+    return line
+
+
+def run_table(a) -> None:
+    """Every row of the measurement table, GPU beside the oracle on this host's
+    cores (the CPU legs run the oracle, oracle/oracle.c, as the reference's CPU
+    path restated; medians of up to 20 runs after up to 5 warm-ups within a
+    time bound per row):
+      C1  M31 forward + inverse, n = 2^16, one column
+      C2  BabyBear forward + inverse, log n 10..24, one column (a single column
+          does not split across cores, so the CPU leg is one thread)
+      C3  BabyBear coset LDE 2^20 x 256, 2x and 4x, fused and unfused (CPU: one
+          column on one thread scaled to 256; all cores on a column sample)
+      C4  uneven batch: plain per-polynomial loop vs one graph launch (CPU: one
+          column of every polynomial on one thread, scaled by its columns)
+      C5  served stream vs the plain loop (see served_sweep)."""
+    import copy
+    import torch
+    import sfntt
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    ctx = sfntt.Context(0)
+    threads = O.default_threads()
+    peak, _ = peaks()
+
+    def cpu_median_ms(fn, budget_s=3.0):
+        t = time.perf_counter()
+        fn()
+        first = time.perf_counter() - t
+        reps = int(max(1, min(20, budget_s / max(first, 1e-6))))
+        for _ in range(min(5, reps // 4)):
+            fn()
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t)
+        return statistics.median(ts) * 1e3
+
+    res = {"cores": threads}
+    sweep = secondary_metrics(ctx, sfntt, torch)
+    x16 = O.lcg(1 << 16, 12345 + (1 << 16), O.M31_P)
+    res["C1"] = {"gpu_us": sweep["m31"]["16"]["fwd_inv_us"],
+                 "cpu_1t_us": cpu_median_ms(lambda: O.m31_inverse(O.m31_forward(x16))) * 1e3,
+                 "gpu_hbm_frac": sweep["m31"]["16"]["hbm_frac"], "note": "L2-resident"}
+    c2 = {}
+    for log_n in range(10, 25):
+        x = O.lcg(1 << log_n, 7 + log_n, O.BB_P, monty=True)
+        g = sweep["bb"][str(log_n)]
+        c2[str(log_n)] = {"gpu_us": g["fwd_inv_us"], "gpu_gelem_s": g["gelem_s"], "gpu_hbm_frac": g["hbm_frac"],
+                          "cpu_1t_us": cpu_median_ms(lambda: O.bb_inverse(O.bb_forward(x)), 2.0) * 1e3}
+    res["C2"] = c2
+    # C3
+    n = 1 << 20
+    xin = torch.randint(0, BB_P, (256 * n,), dtype=torch.int64, device="cuda").to(torch.int32)
+    stream = torch.cuda.current_stream().cuda_stream
+    c3 = {}
+    for added in (1, 2):
+        out = torch.empty(256 * (n << added), dtype=torch.int32, device="cuda")
+        row = {}
+        for fused in (True, False):
+            lde = sfntt.CosetLdeBatch(ctx, fused=fused)
+            ctx.prepare_lde(sfntt.FIELD_BABYBEAR, 20, added, shift_monty(a))
+            f = lambda: lde.execute_dev(xin.data_ptr(), out.data_ptr(), 20, 256, added,
+                                        shift_monty=shift_monty(a), stream=stream)
+            for _ in range(3):
+                f()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(10):
+                f()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 10
+            row["gpu_fused_ms" if fused else "gpu_unfused_ms"] = ms
+        row["gpu_hbm_frac"] = 4 * 256 * n * (1 + (1 << added)) / (row["gpu_fused_ms"] * 1e-3) / (peak * 1e9)
+        b = copy.copy(a)
+        b.log_n, b.batch, b.added_bits = 20, 256, added
+        cpu = cpu_lde_sample(b, 12.0)
+        row["cpu_all_cores_ms"] = cpu["value"]
+        row["cpu_1t_ms"] = cpu["single_thread_ms_full"]
+        c3[f"{1 << added}x"] = row
+        del out
+        torch.cuda.empty_cache()
+    res["C3"] = c3
+    del xin
+    torch.cuda.empty_cache()
+    # C4
+    un = uneven_metrics(a, ctx, sfntt, torch)
+    items = sfntt.uneven_workload(64, seed=2024)
+    cpu_1t = 0.0
+    for k, it in enumerate(items):
+        bb = it["field"] == sfntt.FIELD_BABYBEAR
+        col = O.lcg(1 << it["log_n"], 500 + k, O.BB_P if bb else O.M31_P, monty=bb)
+        t = time.perf_counter()
+        if bb:
+            O.bb_coset_lde(col, it["log_n"], 1, it["added_bits"], threads=1)
+        else:
+            O.m31_lde(col, it["log_n"], 1, it["added_bits"], threads=1)
+        cpu_1t += (time.perf_counter() - t) * it["batch"]
+    res["C4"] = {"gpu_plain_ms": un["plain_loop_ms"], "gpu_graph_ms": un["graph_ms"], "gpu_hbm_frac": un["hbm_frac"],
+                 "outputs_identical": un["outputs_identical"], "cpu_1t_ms": cpu_1t * 1e3}
+    # C5
+    sv = served_sweep(a, ctx, sfntt, torch)
+    res["C5"] = {"at_max_rate": sv["at_max_rate"],
+                 "sweep": [{"rate": r["rate_req_s"], "plain_p50_ms": r["plain"]["p50_ms"],
+                            "plain_p99_ms": r["plain"]["p99_ms"], "served_p50_ms": r["served"]["p50_ms"],
+                            "served_p99_ms": r["served"]["p99_ms"], "plain_melem_s": r["plain"]["melem_per_s"],
+                            "served_melem_s": r["served"]["melem_per_s"], "hbm_frac": r["served"]["hbm_frac"]}
+                           for r in sv["sweep"]]}
+    print(json.dumps({"metric": "measurement table (C1-C5)", "rows": res, "device": ctx.device_info()}), flush=True)
 
 
 def kernel_butterflies(name: str, bytes_per_launch: int, added_bits: int) -> float:
