@@ -205,6 +205,18 @@ inline Status launch_check(sfntt_ctx* ctx, const char* what, cudaStream_t s = nu
   return {};
 }
 
+// Raises a kernel's dynamic shared-memory limit once per device (the
+// attribute stays with the function on that device); `done` is a static owned
+// by the caller's launch function, one per kernel instantiation.
+template <class Kernel>
+inline Status smem_limit_once(Kernel kern, int bytes, int device, std::atomic<uint64_t>& done) {
+  const uint64_t bit = 1ull << (device & 63);
+  if (done.load(std::memory_order_acquire) & bit) return {};
+  SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.fetch_or(bit, std::memory_order_release);
+  return {};
+}
+
 inline bool capturing(cudaStream_t s) {
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {

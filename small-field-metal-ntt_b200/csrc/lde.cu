@@ -119,7 +119,8 @@ Status launch_expand(sfntt_ctx* ctx, const ExpandArgs& ea, uint32_t tiles, cudaS
   using X = Expand<KD, P, LT>;
   constexpr int smem = X::SMEM_WORDS * 4;
   auto kern = expand_kernel<KD, P, LT>;
-  if (smem > 48 * 1024) SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  static std::atomic<uint64_t> smem_done{0};
+  if (smem > 48 * 1024) SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   launch_begin(ctx, s);
   kern<<<tiles, X::NT, smem, s>>>(ea);
   // reads 2^CB points per tile, writes 2^(CB + added_bits)
@@ -198,7 +199,8 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   a.scale_ws = (uint32_t)(((uint64_t)scale_w << 32) / F::P);
   constexpr int smem = 3 * (int)X::TBYTES + 16 + 16 * (int)X::Inv::TW_ENTRIES + 1024;
   auto kern = tma_expand_kernel<F, P, PLAIN>;
-  SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  static std::atomic<uint64_t> smem_done{0};
+  SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, X::NT, smem, s>>>(min, mout, a);

@@ -37,7 +37,8 @@ Status launch_pass(sfntt_ctx* ctx, const PassArgs& a, uint32_t tiles, cudaStream
   using PS = Pass<F, DESC, KD, P, LT, R>;
   constexpr int smem = PS::SMEM_WORDS * 4;
   auto kern = pass_kernel<F, DESC, KD, P, LT, R>;
-  if (smem > 48 * 1024) SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  static std::atomic<uint64_t> smem_done{0};
+  if (smem > 48 * 1024) SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   launch_begin(ctx, s);
   kern<<<tiles, PS::NT, smem, s>>>(a);
   const uint64_t bytes = (uint64_t)tiles << (CB + 3);  // every point read once and written once

@@ -108,7 +108,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   }
   constexpr int smem = 2 * (int)T::TBYTES + 16 + 8 * (int)T::TW_ENTRIES + 1024;
   auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW>;
-  SFNTT_CU(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  static std::atomic<uint64_t> smem_done{0};
+  SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, 2u * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, T::NT, smem, s>>>(min, mout, a);
