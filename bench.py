@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--added-bits", type=int, default=1)
     ap.add_argument("--mode", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--field", default="bb", choices=["bb", "m31"],
+                    help="bb: the BabyBear coset LDE (the headline); m31: the M31 blow-up of the same shape")
     ap.add_argument("--shift", default="31", choices=["31", "reference"],
                     help="coset shift: g = 31 (the multiplicative generator) or the reference's default "
                          "two_adic_generator(log_n_ext + 1); the cost is the same")
@@ -73,7 +75,20 @@ def shift_monty(a) -> int:
     return (31 << 32) % BB_P  # to_monty(31) = 31 * 2^32 mod p
 
 
+def metric_name(a) -> str:
+    if a.field == "m31":
+        return f"M31 blow-up 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
+    return METRIC if (a.log_n, a.batch, a.added_bits) == (20, 256, 1) else \
+        f"BabyBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
+
+
 def workload(a) -> dict:
+    if a.field == "m31":
+        return {"workload": f"M31 blow-up 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x (inverse on odds(log n), "
+                            f"zero-pad, forward on odds(log n + added_bits))",
+                "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "layout": "SoA column-major, u32",
+                "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
+                      f"{4 * a.batch << (a.log_n + a.added_bits) >> 20} MiB out per step)"}
     return {"workload": f"BabyBear coset LDE 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x blow-up",
             "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
             "shift": "g = 31, row i times 31^i" if a.shift == "31" else
@@ -162,24 +177,37 @@ def ncu_traffic(kernel: str):
 
 
 # ------------------------------------------------------------ CPU legs ---
+def field_p(a) -> int:
+    return BB_P if a.field == "bb" else 2147483647
+
+
+def oracle_lde(a, O):
+    """The oracle's LDE of the bench's field: f(x, columns, threads)."""
+    if a.field == "m31":
+        return lambda x, cols, threads: O.m31_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+    return lambda x, cols, threads: O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a),
+                                                   threads=threads)
+
+
 def cpu_lde_sample(a, target_s: float) -> dict:
     """The oracle (reference CPU path restated in C) on a bounded column
     sample, all host threads; returns ms scaled to the full column count."""
     from oracle import oracle as O
     threads = O.default_threads()
     n = 1 << a.log_n
-    one = O.lcg(n, 1, BB_P, monty=True)
+    lde = oracle_lde(a, O)
+    one = O.lcg(n, 1, field_p(a), monty=a.field == "bb")
     t = time.perf_counter()
-    O.bb_coset_lde(one, a.log_n, 1, a.added_bits, shift_monty=shift_monty(a), threads=1)
+    lde(one, 1, 1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(target_s * threads / max(t1, 1e-6)))))
     cols = max(1, min(a.batch, (cols // threads) * threads or cols))
-    x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field == "bb")
     t = time.perf_counter()
-    O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a), threads=threads)
+    lde(x, cols, threads)
     ts = time.perf_counter() - t
     return {"value": ts * 1e3 * a.batch / cols, "unit": "ms", "cores": threads, "kind": "port",
-            "sample": f"{cols} of {a.batch} columns (oracle/oracle.c coset_lde, OpenMP over columns), "
+            "sample": f"{cols} of {a.batch} columns (oracle/oracle.c LDE, OpenMP over columns), "
                       f"scaled x{a.batch / cols:.2f}; 1-thread column time {t1 * 1e3:.1f} ms",
             "single_thread_ms_full": t1 * 1e3 * a.batch}
 
@@ -191,22 +219,24 @@ def run_reference(a, rank: int) -> None:
     threads = O.default_threads()
     n = 1 << a.log_n
     per_step = max(0.3, min(20.0, 150.0 / max(1, a.steps + a.warmup)))  # whole run ~2.5 min
+    lde = oracle_lde(a, O)
     t = time.perf_counter()
-    O.bb_coset_lde(O.lcg(n, 1, BB_P, monty=True), a.log_n, 1, a.added_bits, shift_monty=shift_monty(a), threads=1)
+    lde(O.lcg(n, 1, field_p(a), monty=a.field == "bb"), 1, 1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(per_step * threads / max(t1, 1e-6)))))
-    x = O.lcg(cols << a.log_n, 42 + a.log_n, BB_P, monty=True)
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field == "bb")
     times = []
     for i in range(a.warmup + a.steps):
         t = time.perf_counter()
-        O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a), threads=threads)
+        lde(x, cols, threads)
         if i >= a.warmup:
             times.append((time.perf_counter() - t) * a.batch / cols)
     ms = statistics.mean(times) * 1e3
     sample = f"{cols} of {a.batch} columns per step (oracle/oracle.c, OpenMP over columns), scaled x{a.batch / cols:.2f}"
-    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": ms / PUBLISHED_MS, "dtype": "u32 (BabyBear Montgomery)", "data": "synthetic",
+    line = {"impl": "reference", "metric": metric_name(a), "value": ms, "unit": "ms", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": ms / PUBLISHED_MS if metric_name(a) == METRIC else None,
+            "dtype": "u32 (BabyBear Montgomery)" if a.field == "bb" else "u32 (M31 canonical)", "data": "synthetic",
             "config": workload(a),
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -238,19 +268,34 @@ def main() -> None:
     barrier, max_all = rep.barrier, rep.max
 
     ctx = sfntt.Context(local)
-    lde = sfntt.CosetLdeBatch(ctx, fused=(a.mode == "fused"))
+    m31 = a.field == "m31"
     n, n_ext = 1 << a.log_n, 1 << (a.log_n + a.added_bits)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(1234 + rank)
-    x = torch.randint(0, BB_P, (a.batch * n,), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    x = torch.randint(0, field_p(a), (a.batch * n,), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
     out = torch.empty(a.batch * n_ext, dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
     shift = shift_monty(a)
-    ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, shift)
+    if m31:
+        lde = sfntt.M31Lde(ctx)
+        ctx.prepare_lde(sfntt.FIELD_M31, a.log_n, a.added_bits)
 
-    def step():
-        lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, shift_monty=shift, stream=stream)
+        def step():
+            lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream)
+
+        def host_call(hin, hout):
+            lde.execute(hin, a.log_n, a.batch, a.added_bits, out=hout)
+    else:
+        lde = sfntt.CosetLdeBatch(ctx, fused=(a.mode == "fused"))
+        sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
+        ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, shift)
+
+        def step():
+            lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, shift_monty=shift,
+                            stream=stream)
+
+        def host_call(hin, hout):
+            lde.execute(hin, a.log_n, a.batch, a.added_bits, shift_monty=shift, out=hout)
 
     for _ in range(a.warmup):
         step()
@@ -311,24 +356,25 @@ def main() -> None:
         hin = ctx.pinned(a.batch * n)
         hout = ctx.pinned(a.batch * n_ext)
         hin.array[:] = x.cpu().numpy().view("uint32")
-        lde.execute(hin.array, a.log_n, a.batch, a.added_bits, shift_monty=shift, out=hout.array)  # warm-up
+        host_call(hin.array, hout.array)  # warm-up
         barrier()
         ts = []
         for _ in range(a.e2e_steps):
             t = time.perf_counter()
-            lde.execute(hin.array, a.log_n, a.batch, a.added_bits, shift_monty=shift, out=hout.array)
+            host_call(hin.array, hout.array)
             ts.append(time.perf_counter() - t)
         e2e_ms = max_all(statistics.mean(ts) * 1e3)
         ok = bool((hout.array[: n_ext] == out[: n_ext].cpu().numpy().view("uint32")).all())
         e2e = {"value": e2e_ms / world, "unit": "ms", "h2d_bytes_per_step": 4 * a.batch * n,
                "d2h_bytes_per_step": 4 * a.batch * n_ext, "steps": a.e2e_steps,
-               "path": "sfntt_bb_coset_lde (pinned host buffers, column chunks pipelined over 3 streams)",
+               "path": ("sfntt_m31_lde" if m31 else "sfntt_bb_coset_lde") +
+                       " (pinned host buffers, column chunks pipelined over 3 streams)",
                "matches_device_run": ok}
         hin.free()
         hout.free()
 
     secondary = None if a.no_secondary else secondary_metrics(ctx, sfntt, torch)
-    layouts = None if a.no_secondary else layout_metrics(a, ctx, sfntt, torch, x, out, stream)
+    layouts = None if (a.no_secondary or m31) else layout_metrics(a, ctx, sfntt, torch, x, out, stream)
     del x, out
     torch.cuda.empty_cache()
     served = None if (a.no_served or world > 1) else served_sweep(a, ctx, sfntt, torch)
@@ -340,10 +386,11 @@ def main() -> None:
     rep.close()
     if rank != 0:
         return
-    line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
+    line = {"metric": metric_name(a), "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": value / PUBLISHED_MS, "dtype": "u32 (BabyBear Montgomery, exact)",
-            "data": "synthetic: seeded uniform canonical values in [0, p), Montgomery on device",
+            "vs_baseline": value / PUBLISHED_MS if metric_name(a) == METRIC else None,
+            "dtype": "u32 (M31 canonical, exact)" if m31 else "u32 (BabyBear Montgomery, exact)",
+            "data": "synthetic: seeded uniform canonical values in [0, p)" + ("" if m31 else ", Montgomery on device"),
             "config": {**workload(a), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "gpu_launches": launches, "launches_per_step": launches / a.steps,
             "lde_gbs": lde_gbs, "lde_hbm_frac": lde_gbs / peak,

@@ -396,9 +396,10 @@ class M31Lde:
     def __init__(self, ctx: Context | None = None, device: int = 0):
         self.ctx = ctx or default_context(device)
 
-    def execute(self, input, log_n: int, batch_size: int, added_bits: int) -> LdeResult:
+    def execute(self, input, log_n: int, batch_size: int, added_bits: int,
+                out: np.ndarray | None = None) -> LdeResult:
         inp = _u32(input)
-        dst = np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
+        dst = out if out is not None else np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
         ns = ctypes.c_uint64()
         st = _ffi.lib().sfntt_m31_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits,
                                       _p(dst), ctypes.byref(ns))
