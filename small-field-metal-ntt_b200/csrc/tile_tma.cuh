@@ -280,6 +280,57 @@ struct TPass {
     }
   }
 
+  // ---- synchronisation of an exchange ----
+  // A word written in round kp's layout is read in round k's layout by the
+  // thread that owns it there.  Tile bits that are thread bits in both layouts
+  // pin the owner's thread-id bits; when they sit at the same thread-id
+  // position in both, writer and reader agree on those bits, so only threads
+  // that share them exchange data.  If the pinned bits cover every warp bit
+  // the exchange stays inside a warp (__syncwarp); if they cover some, inside
+  // the warps that share them (a named barrier per group); else the CTA.
+  __host__ __device__ static constexpr int tid_bit(int k, int c) {
+    const RoundMap mp = make_map<KD, P, LT, R>(k);
+    for (int g = 0; g < mp.ngrp; ++g) {
+      const int t = c - mp.gshift[g];
+      if (t >= 0 && t < 32 && ((mp.gmask[g] >> t) & 1u)) return t;
+    }
+    return -1;
+  }
+  template <int kp, int k>
+  __host__ __device__ static constexpr int xfixed() {
+    int mask = 0;
+    for (int c = 0; c < CB; ++c) {
+      const int a = tid_bit(kp, c), b = tid_bit(k, c);
+      if (a >= 0 && b >= 0) {
+        if (a != b) return -1;
+        mask |= 1 << a;
+      }
+    }
+    return mask;
+  }
+  static constexpr int kWarpBits = (NT - 1) & ~31;
+  template <int kp, int k>
+  __device__ static __forceinline__ void xsync(uint32_t tid) {
+    constexpr int fixed = xfixed<kp, k>();
+    constexpr int wf = fixed < 0 ? 0 : (fixed & kWarpBits);
+    if constexpr (fixed >= 0 && kWarpBits != 0 && wf == kWarpBits) {
+      __syncwarp();
+    } else if constexpr (wf != 0 && __builtin_popcount(wf) <= 3) {
+      uint32_t id = 1, i = 0;
+#pragma unroll
+      for (int bit = 5; bit < 16; ++bit) {
+        if ((wf >> bit) & 1) {
+          id += ((tid >> bit) & 1u) << i;
+          ++i;
+        }
+      }
+      constexpr uint32_t count = (uint32_t)NT >> __builtin_popcount(wf);
+      asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+    } else {
+      __syncthreads();
+    }
+  }
+
   // All K rounds starting from registers in round (DESC ? K-1 : 0)'s layout,
   // exchanging through `buf`; ends in round (DESC ? 0 : K-1)'s layout.
   template <int i>
@@ -290,7 +341,7 @@ struct TPass {
       if constexpr (i > 0) {
         constexpr int kp = DESC ? (K - i) : (i - 1);
         st<kp>(buf, v, tid);
-        __syncthreads();
+        xsync<kp, k>(tid);
         ld<k>(buf, v, tid);
       }
       round<k>(v, a, tws, g, tid);
@@ -395,6 +446,13 @@ struct TPass {
     if (tid == 0) tma::wait_all();
   }
 };
+
+// Exchange groups of the 12- and 8-layer contiguous passes and the 8-layer
+// strided pass (checked against a brute-force walk over every tile word).
+static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<2, 1>() == 0x10F, "C12 2->1: tid bits 0-3, 8");
+static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<1, 0>() == 0x1F0, "C12 1->0: tid bits 4-8 (in a warp)");
+static_assert(TPass<BabyBear, false, Kind::C, 8>::xfixed<0, 1>() == 0x1F0, "C8 0->1: in a warp");
+static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: lanes only, whole CTA");
 
 template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
 __global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW>::NT, 2)
