@@ -175,11 +175,11 @@ __global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, 
 }
 
 // mul: BabyBear multiplier table M_q; scale_w: M31's n^-1 (canonical).
-template <class F, int P, bool PLAIN>
+template <class F, int P, bool PLAIN, bool LSTAGE = false>
 Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_stride, uint32_t* d_out, uint32_t log_n,
                          uint32_t batch, uint32_t added_bits, const uint2* tw_inv, const uint2* tw_fwd,
                          const uint2* mul, cudaStream_t s, uint32_t scale_w = 0) {
-  using X = TExpand<F, P, PLAIN>;
+  using X = TExpand<F, P, PLAIN, LSTAGE>;
   const uint32_t lo = log_n - P;
   const uint64_t n = 1ull << log_n, n_ext = n << added_bits;
   CUtensorMap min, mout;
@@ -197,15 +197,16 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   a.ntiles = (uint32_t)(((uint64_t)batch * n) >> (P + 5));
   a.scale_w = scale_w;
   a.scale_ws = (uint32_t)(((uint64_t)scale_w << 32) / F::P);
-  constexpr int smem = 3 * (int)X::TBYTES + 16 + 16 * (int)X::Inv::TW_ENTRIES + 1024;
-  auto kern = tma_expand_kernel<F, P, PLAIN>;
+  constexpr int smem = 3 * (int)X::TBYTES + 16 + 16 * (int)X::TW_ENTRIES + 1024;
+  auto kern = tma_expand_kernel<F, P, PLAIN, LSTAGE>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   kern<<<grid, X::NT, smem, s>>>(min, mout, a);
   static const std::string name =
-      std::string(F::kMontgomery ? "bb" : "m31") + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "");
+      std::string(F::kMontgomery ? "bb" : "m31") + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "") +
+      (LSTAGE ? "c" : "");
   return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
 }
 
@@ -247,6 +248,9 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
       if (plain)
         SFNTT_TRY((launch_tma_expand<BabyBear, 8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
                                                         tw_fwd, mul, s)));
+      else if (batch >= 16)  // the chunk's twiddles are reused across >= 16 columns
+        SFNTT_TRY((launch_tma_expand<BabyBear, 8, false, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits,
+                                                               tw_inv, tw_fwd, mul, s)));
       else
         SFNTT_TRY((launch_tma_expand<BabyBear, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
                                                          tw_fwd, mul, s)));

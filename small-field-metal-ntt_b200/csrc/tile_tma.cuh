@@ -78,9 +78,13 @@ struct TileCoord {
 // lane-independent twiddles from shared memory and leave the four-step twist to
 // the neighbouring pass; otherwise use the reference's per-position twiddles
 // tw[L][pos mod 2^L] from the global table.  TW: this pass applies a boundary
-// twist (forward: at load, inverse: at store).
-template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false>
+// twist (forward: at load, inverse: at store).  LSTAGE (BabyBear Kind::S,
+// per-position twiddles): the caller has staged the twiddles of the tile's
+// 32-position chunk in shared memory (see lchunk_entry), so every twiddle is a
+// shared-memory load instead of an L2 one.
+template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false, bool LSTAGE = false>
 struct TPass {
+  static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN), "chunk staging: BabyBear strided only");
   static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
   static constexpr int CB = P + LT;
   static constexpr int R = 4;
@@ -150,6 +154,9 @@ struct TPass {
       const uint32_t mask = (1u << beta) - 1u;
       if constexpr (KD == Kind::C) return base[(ct & mask) + (cm & mask)];
       else return base[((ct >> 5) & mask) + ((cm >> 5) & mask)];
+    } else if constexpr (LSTAGE) {  // tw[L][pos mod 2^L] from the chunk's staged copy
+      const uint32_t em = (1u << beta) - 1u;
+      return tws[32u * em + ((((ct >> 5) & em) + ((cm >> 5) & em)) << 5) + (ct & 31u)];
     } else if constexpr (F::kMontgomery) {  // BabyBear strided, per position: tw[L][pos mod 2^L]
       const uint2* base = a.tw + ((1u << L) - 1u);
       const uint32_t em = (1u << beta) - 1u;
@@ -387,6 +394,21 @@ struct TPass {
     for (uint32_t i = tid; i < TW_ENTRIES; i += NT) dst[i] = __ldg(src + i);
   }
 
+  // Per-position twiddles of one 32-position chunk of strided tiles (layers
+  // lo .. lo+P-1): entry 32 (2^beta - 1) + (e_low << 5) + u holds
+  // tw[lo + beta][(e_low << lo) + chunk * 32 + u] for e_low < 2^beta, u < 32.
+  static constexpr uint32_t LCHUNK_ENTRIES = 32u * ((1u << P) - 1u);
+  __device__ static __forceinline__ void stage_lchunk(uint2* dst, const uint2* src, uint32_t lo, uint32_t chunk,
+                                                      uint32_t tid) {
+    for (uint32_t i = tid; i < LCHUNK_ENTRIES; i += NT) {
+      const uint32_t row = (i >> 5) + 1u;  // 2^beta + e_low
+      const uint32_t beta = 31u - __clz(row);
+      const uint32_t e_low = row - (1u << beta);
+      const uint32_t L = lo + beta;
+      dst[i] = __ldg(src + ((1u << L) - 1u) + ((uint64_t)e_low << lo) + (chunk << 5) + (i & 31u));
+    }
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
@@ -471,12 +493,17 @@ tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__
 //     are a plain replication (CT butterfly on (a, 0) gives (a, a)), so every
 //     block starts from the same values.
 // The inverse result stays in registers across the blocks.
-template <class F, int P, bool PLAIN>
+// LSTAGE (BabyBear, per-position twiddles): each CTA takes a contiguous range
+// of tiles; tiles are numbered column-fastest, so consecutive tiles share a
+// 32-position chunk and its twiddles, which are staged in shared memory
+// (both directions, 2 x 64 KB for P = 8) whenever the chunk changes.
+template <class F, int P, bool PLAIN, bool LSTAGE = false>
 struct TExpand {
-  using Inv = TPass<F, false, Kind::S, P, PLAIN>;
-  using Fwd = TPass<F, true, Kind::S, P, PLAIN>;
+  using Inv = TPass<F, false, Kind::S, P, PLAIN, false, LSTAGE>;
+  using Fwd = TPass<F, true, Kind::S, P, PLAIN, false, LSTAGE>;
   static constexpr int K = Inv::K, E = Inv::E, NT = Inv::NT, R = Inv::R, LT = Inv::LT;
   static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
+  static constexpr uint32_t TW_ENTRIES = LSTAGE ? Inv::LCHUNK_ENTRIES : Inv::TW_ENTRIES;  // per direction
   static_assert(F::kMontgomery || !PLAIN, "M31 passes have no plain variant");
 
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
@@ -487,11 +514,21 @@ struct TExpand {
     uint32_t* ostage = stage + 2 * TWORDS;
     uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 3 * TWORDS);
     uint2* tws_inv = reinterpret_cast<uint2*>(bar + 2);
-    uint2* tws_fwd = tws_inv + Inv::TW_ENTRIES;
+    uint2* tws_fwd = tws_inv + TW_ENTRIES;
     const uint32_t tid = threadIdx.x;
     const TmaArgs& ai = args;
-    uint32_t t = blockIdx.x;
-    if (t >= ai.ntiles) return;
+    uint32_t t, t_end, t_step;
+    if constexpr (LSTAGE) {  // contiguous range per CTA
+      const uint32_t per = (ai.ntiles + gridDim.x - 1) / gridDim.x;
+      t = blockIdx.x * per;
+      t_end = (t + per < ai.ntiles) ? t + per : ai.ntiles;
+      t_step = 1;
+    } else {
+      t = blockIdx.x;
+      t_end = ai.ntiles;
+      t_step = gridDim.x;
+    }
+    if (t >= t_end) return;
     if constexpr (PLAIN) {
       Inv::stage_twiddles(tws_inv, ai.tw, tid);
       Fwd::stage_twiddles(tws_fwd, ai.tw_fwd, tid);
@@ -514,20 +551,31 @@ struct TExpand {
     const uint32_t n = 1u << ai.log_n;
     const uint32_t nq = 1u << ai.log_q;
     uint32_t x[E], v[E];
-    for (uint32_t it = 0; t < ai.ntiles; t += gridDim.x, ++it) {
+    uint32_t staged = ~0u;  // chunk whose twiddles are in shared memory (LSTAGE)
+    for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
       const uint32_t buf = it & 1u;
       uint32_t* cur = stage + buf * TWORDS;
-      const uint32_t tn = t + gridDim.x;
-      if (tid == 0 && tn < ai.ntiles) {
+      const uint32_t tn = t + t_step;
+      if (tid == 0 && tn < t_end) {
         tma::wait_reads();
         tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
         Inv::tma_load(min, Inv::geo(ai, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+      }
+      if constexpr (LSTAGE) {
+        // Every thread passed the previous tile's last barrier after its last
+        // twiddle read; the barrier below publishes the new copy.
+        const uint32_t chunk = (t / ai.batch) & ((1u << (ai.lo - 5)) - 1u);
+        if (chunk != staged) {
+          Inv::stage_lchunk(tws_inv, ai.tw, ai.lo, chunk, tid);
+          Fwd::stage_lchunk(tws_fwd, ai.tw_fwd, ai.lo, chunk, tid);
+          staged = chunk;
+        }
       }
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(ai.err, 1);
-          if (tn < ai.ntiles) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
           tma::wait_all();
         }
         return;
@@ -581,10 +629,10 @@ struct TExpand {
   }
 };
 
-template <class F, int P, bool PLAIN>
-__global__ void __launch_bounds__(TExpand<F, P, PLAIN>::NT, 1)
+template <class F, int P, bool PLAIN, bool LSTAGE>
+__global__ void __launch_bounds__(TExpand<F, P, PLAIN, LSTAGE>::NT, 1)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
-  TExpand<F, P, PLAIN>::run(&min, &mout, a);
+  TExpand<F, P, PLAIN, LSTAGE>::run(&min, &mout, a);
 }
 
 }  // namespace sfntt

@@ -219,7 +219,10 @@ def test_batch_equals_single(ctx, field, log_n, batch):
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("log_n,batch,added", [(8, 4, 1), (12, 8, 1), (8, 4, 2), (0, 3, 1), (1, 2, 2), (5, 3, 3),
                                                 (13, 2, 1), (14, 3, 2), (16, 4, 1), (18, 2, 1), (11, 5, 4),
-                                                (6, 2, 5)])
+                                                (6, 2, 5),
+                                                # >= 16 columns: chunk-staged twiddles in the fused expand,
+                                                # chunk changes inside a CTA's tile range
+                                                (13, 16, 1), (14, 24, 2), (15, 17, 1), (16, 33, 3), (17, 16, 4)])
 def test_coset_lde_matches_cpu(ctx, fused, log_n, batch, added):
     lde = sfntt.CosetLdeBatch(ctx, fused=fused)
     x = O.lcg(batch << log_n, 42, O.BB_P, monty=True)
