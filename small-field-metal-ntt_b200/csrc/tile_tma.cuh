@@ -506,6 +506,13 @@ struct TExpand {
   static constexpr uint32_t TW_ENTRIES = LSTAGE ? Inv::LCHUNK_ENTRIES : Inv::TW_ENTRIES;  // per direction
   static_assert(F::kMontgomery || !PLAIN, "M31 passes have no plain variant");
 
+  // Multipliers M_q of the thread's 16 slots (round K-1 layout) from mq = M_q + pos_t.
+  __device__ static __forceinline__ void load_mul(uint2 (&w)[E], const uint2* mq, uint32_t lo) {
+    using M = RM<Kind::S, P, LT, R, K - 1>;
+#pragma unroll
+    for (int m = 0; m < E; ++m) w[m] = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
@@ -581,14 +588,18 @@ struct TExpand {
         return;
       }
       const typename Inv::Geo g = Inv::geo(ai, t);
+      // position of slot m: pos_base + u + (e << lo)
+      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
+      // BabyBear multipliers are software-pipelined: block q+1's are loaded
+      // while block q's forward layers run (block 0's during the inverse).
+      uint2 w[F::kMontgomery ? E : 1];
+      if constexpr (F::kMontgomery) load_mul(w, ai.mul + pos_t, lo);
       Inv::template ld<0>(cur, x, tid);
       Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
       if constexpr (!F::kMontgomery) {
 #pragma unroll
         for (int m = 0; m < E; ++m) x[m] = mul_shoup<F>(x[m], ai.scale_w, ai.scale_ws);  // n^-1
       }
-      // position of slot m: pos_base + u + (e << lo)
-      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
       for (uint32_t q = 0; q < nq; ++q) {
         uint32_t* ob = (q & 1u) ? ostage : cur;
         // The TMA store that last read ob is the one before the newest pending
@@ -599,12 +610,9 @@ struct TExpand {
           __syncthreads();
         }
         if constexpr (F::kMontgomery) {
-          const uint2* mq = ai.mul + (uint64_t)q * n + pos_t;
 #pragma unroll
-          for (int m = 0; m < E; ++m) {
-            const uint2 w = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
-            v[m] = mul_shoup<F>(x[m], w.x, w.y);
-          }
+          for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
+          if (q + 1 < nq) load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);
         } else {
 #pragma unroll
           for (int m = 0; m < E; ++m) v[m] = x[m];
