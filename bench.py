@@ -304,7 +304,6 @@ def main() -> None:
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     sampler = ClockSampler(gpu_id)
     time.sleep(0.6)
-    ctx.kernel_timing(True)
     launches0 = ctx.launch_count()
     barrier()
     torch.cuda.synchronize()
@@ -318,9 +317,15 @@ def main() -> None:
     w1 = time.time()
     barrier()
     launches = ctx.launch_count() - launches0
+    clocks = sampler.stop(w0, w1)
+    # per-kernel breakdown on a separate run: events around every launch
+    # would stop consecutive passes from overlapping their launch gaps
+    ctx.kernel_timing(True)
+    for _ in range(min(20, a.steps)):
+        step()
+    torch.cuda.synchronize()
     kt = ctx.kernel_times()
     ctx.kernel_timing(False)
-    clocks = sampler.stop(w0, w1)
     step_ms = max_all(ev0.elapsed_time(ev1) / a.steps)
     value = job_time_per_unit(step_ms, world)
 
@@ -719,11 +724,13 @@ def kernel_butterflies(name: str, bytes_per_launch: int, added_bits: int) -> flo
 def secondary_metrics(ctx, sfntt, torch) -> dict:
     """The single-column NTT configurations: BabyBear forward + inverse for
     log n = 10..24 and the M31 Circle NTT likewise (n = 2^16 is the M31
-    configuration), values uniform in [0, p), device-resident, 50 timed pairs
-    after 5 warm-up pairs.  Columns up to 2^24 words (64 MiB) stay resident in
+    configuration), values uniform in [0, p), device-resident; 10 forward +
+    inverse pairs captured in a CUDA graph, replayed 10 times after 5 warm-up
+    pairs, so small sizes measure the device rather than the host's launch rate.  Columns up to 2^24 words (64 MiB) stay resident in
     the 126 MB L2 across repetitions, so the byte fraction is against HBM
     bandwidth for reference only.  Gelem/s counts n per transform."""
-    res = {"note": "forward+inverse pairs on one device-resident column (L2-resident up to 2^24)"}
+    res = {"note": "forward+inverse pairs on one device-resident column (L2-resident up to 2^24), "
+                   "replayed from a CUDA graph"}
     stream = torch.cuda.current_stream().cuda_stream
     peak, _ = peaks()
     for field, name in ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31")):
@@ -736,15 +743,24 @@ def secondary_metrics(ctx, sfntt, torch) -> dict:
             for _ in range(5):
                 b.forward_dev(d.data_ptr(), log_n, 1, stream)
                 b.inverse_dev(d.data_ptr(), log_n, 1, stream)
-            reps = 50
+            torch.cuda.synchronize()
+            # 10 pairs captured once and replayed: device time, not Python's launch rate
+            graph, per_graph = torch.cuda.CUDAGraph(), 10
+            with torch.cuda.graph(graph):
+                cs = torch.cuda.current_stream().cuda_stream
+                for _ in range(per_graph):
+                    b.forward_dev(d.data_ptr(), log_n, 1, cs)
+                    b.inverse_dev(d.data_ptr(), log_n, 1, cs)
+            graph.replay()
+            reps = 10
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             for _ in range(reps):
-                b.forward_dev(d.data_ptr(), log_n, 1, stream)
-                b.inverse_dev(d.data_ptr(), log_n, 1, stream)
+                graph.replay()
             e1.record()
             torch.cuda.synchronize()
-            us = e0.elapsed_time(e1) * 1e3 / reps
+            del graph
+            us = e0.elapsed_time(e1) * 1e3 / (reps * per_graph)
             n = 1 << log_n
             rows[str(log_n)] = {"fwd_inv_us": us, "gelem_s": 2 * n / (us * 1e-6) / 1e9,
                                 "gbs": 16 * n / (us * 1e-6) / 1e9, "hbm_frac": 16 * n / (us * 1e-6) / 1e9 / peak}

@@ -203,7 +203,7 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
-  kern<<<grid, X::NT, smem, s>>>(min, mout, a);
+  SFNTT_CU(launch_pdl(kern, grid, X::NT, smem, s, pdl_fits(grid), min, mout, a));
   static const std::string name =
       std::string(F::kMontgomery ? "bb" : "m31") + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "") +
       (LSTAGE ? "c" : "");

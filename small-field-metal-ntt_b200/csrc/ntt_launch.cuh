@@ -40,7 +40,7 @@ Status launch_pass(sfntt_ctx* ctx, const PassArgs& a, uint32_t tiles, cudaStream
   static std::atomic<uint64_t> smem_done{0};
   if (smem > 48 * 1024) SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   launch_begin(ctx, s);
-  kern<<<tiles, PS::NT, smem, s>>>(a);
+  SFNTT_CU(launch_pdl(kern, tiles, PS::NT, smem, s, pdl_fits(tiles), a));
   const uint64_t bytes = (uint64_t)tiles << (CB + 3);  // every point read once and written once
   return launch_check(ctx, pass_name<F, DESC, KD, P>(), s, bytes);
 }

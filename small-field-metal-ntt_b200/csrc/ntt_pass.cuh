@@ -35,6 +35,7 @@
 #include <cstdint>
 
 #include "field.cuh"
+#include "pdl.cuh"
 
 namespace sfntt {
 
@@ -346,6 +347,7 @@ struct Pass {
 template <class F, bool DESC, Kind KD, int P, int LT, int R>
 __global__ void __launch_bounds__(Pass<F, DESC, KD, P, LT, R>::NT)
 pass_kernel(PassArgs a) {
+  pdl_enter();
   Pass<F, DESC, KD, P, LT, R>::run(a);
 }
 

@@ -479,6 +479,7 @@ static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: l
 template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
 __global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW>::NT, 2)
 tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
+  pdl_enter();
   TPass<F, DESC, KD, P, PLAIN, TW>::run(&min, &mout, a);
 }
 
@@ -640,6 +641,7 @@ struct TExpand {
 template <class F, int P, bool PLAIN, bool LSTAGE>
 __global__ void __launch_bounds__(TExpand<F, P, PLAIN, LSTAGE>::NT, 1)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
+  pdl_enter();
   TExpand<F, P, PLAIN, LSTAGE>::run(&min, &mout, a);
 }
 

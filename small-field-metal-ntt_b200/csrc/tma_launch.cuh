@@ -112,7 +112,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t grid = std::min<uint32_t>(a.ntiles, 2u * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
-  kern<<<grid, T::NT, smem, s>>>(min, mout, a);
+  SFNTT_CU(launch_pdl(kern, grid, T::NT, smem, s, pdl_fits(grid), min, mout, a));
   return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
 }
 
