@@ -768,6 +768,29 @@ def secondary_metrics(ctx, sfntt, torch) -> dict:
         best = max(rows.items(), key=lambda kv: kv[1]["gelem_s"])
         res[f"{name}_best_gelem_s"] = {"log_n": int(best[0]), "gelem_s": best[1]["gelem_s"]}
     res["m31_2^16_fwd_inv_us"] = res["m31"]["16"]["fwd_inv_us"]
+    # many small columns (lattice-crypto shapes): 2^24 points per batch
+    lattice = {}
+    for field, name in ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31")):
+        b = (sfntt.BbCudaCtGsR4 if field == sfntt.FIELD_BABYBEAR else sfntt.CudaCtGsR4)(ctx)
+        for log_n in (8, 10):
+            cols = 1 << (24 - log_n)
+            d = torch.randint(0, BB_P, (cols << log_n,), dtype=torch.int64, device="cuda").to(torch.int32)
+            ctx.prepare(field, log_n)
+            for _ in range(3):
+                b.forward_dev(d.data_ptr(), log_n, cols, stream)
+                b.inverse_dev(d.data_ptr(), log_n, cols, stream)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                b.forward_dev(d.data_ptr(), log_n, cols, stream)
+                b.inverse_dev(d.data_ptr(), log_n, cols, stream)
+            e1.record()
+            torch.cuda.synchronize()
+            us = e0.elapsed_time(e1) * 1e3 / 20
+            lattice[f"{name}_2^{log_n}x{cols}"] = {"fwd_inv_us": us, "gelem_s": 2 * (cols << log_n) / (us * 1e-6) / 1e9,
+                                                   "hbm_frac": 16 * (cols << log_n) / (us * 1e-6) / 1e9 / peak}
+    res["many_small_columns"] = lattice
     return res
 
 

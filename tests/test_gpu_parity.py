@@ -215,6 +215,21 @@ def test_batch_equals_single(ctx, field, log_n, batch):
         b.forward_ntt_batch_gpu(x[:-1], log_n, batch)
 
 
+@pytest.mark.parametrize("field", [BB, M31])
+@pytest.mark.parametrize("log_n,batch", [(8, 4096), (10, 1024), (9, 777)])
+def test_many_small_columns(ctx, field, log_n, batch):
+    """Lattice-crypto shapes: thousands of 256..1024-point NTTs in one batch
+    (sampled columns against the oracle, the whole batch round-trips)."""
+    b = (sfntt.BbBatchNtt if field == BB else sfntt.CudaCtGsR4)(ctx)
+    x = data(field, batch << log_n, 300 + log_n)
+    fw, _ = b.forward_ntt_batch_gpu(x, log_n, batch)
+    n = 1 << log_n
+    for c in sorted({0, 1, batch // 3, batch // 2 + 5, batch - 2, batch - 1}):
+        assert np.array_equal(fw[c * n:(c + 1) * n], ofwd(field, x[c * n:(c + 1) * n])), c
+    back, _ = b.inverse_ntt_batch_gpu(fw, log_n, batch)
+    assert np.array_equal(back, x)
+
+
 # ---- coset LDE (src/lde/mod.rs:194-271) ----------------------------------------
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("log_n,batch,added", [(8, 4, 1), (12, 8, 1), (8, 4, 2), (0, 3, 1), (1, 2, 2), (5, 3, 3),
