@@ -82,7 +82,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
       r.contiguous = lo[pi] == 0;
       r.batch = batch;
       r.scale_w = (i == kt - 1) ? scale_w : 0u;
-      ok = tma_pass_ok(r, field == SFNTT_M31);
+      ok = tma_pass_ok(r);
     }
     if (ok && field == SFNTT_BABYBEAR) {
       // Strided passes either use per-position twiddles (self-contained) or,

@@ -165,8 +165,8 @@ struct TPass {
     } else {  // M31: tw[L][pos >> (L+1)]
       const uint32_t n = 1u << a.log_n;
       const uint2* base = a.tw + (n - (n >> L));
-      if constexpr (KD == Kind::C) {  // M31 tiles never span columns (tma_pass_ok)
-        return __ldg(base + ((g.pos_base >> (L + 1)) + (ct >> (L + 1)) + (cm >> (L + 1))));
+      if constexpr (KD == Kind::C) {  // tile bits above log n select the column (spanning tiles)
+        return __ldg(base + ((g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1)) + ((cm & (n - 1u)) >> (L + 1))));
       } else {
         return __ldg(base + ((g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1)) + ((cm >> 5) >> (beta + 1))));
       }
@@ -193,7 +193,7 @@ struct TPass {
         const uint32_t L = a.lo + beta;
         const uint32_t n = 1u << a.log_n;
         const uint2* base = a.tw + (n - (n >> L));
-        if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + (ct >> (L + 1));
+        if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1));
         else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
         uint2 tv[E / 2];
         if (j == r - 1) {

@@ -34,15 +34,16 @@ Status tensor_map_encode(CUtensorMap* map, const void* base, uint32_t rank, cons
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-// Can a pass of this shape run on the TMA engine?  (Per-block M31 twiddles
-// are only supported on tiles inside one column.)
-inline bool tma_pass_ok(const TmaRequest& r, bool per_block) {
+// Can a pass of this shape run on the TMA engine?  Contiguous passes over
+// columns shorter than a tile need dense columns (stride n) whose batch fills
+// whole tiles.
+inline bool tma_pass_ok(const TmaRequest& r) {
   if (!aligned16(r.in) || !aligned16(r.out) || (r.in_stride & 3) || (r.out_stride & 3)) return false;
   const uint64_t n = 1ull << r.log_n;
   if (r.contiguous) {
     if (r.P < 5 || r.P > 12 || r.lo != 0) return false;
     if (n >= kTileWords) return true;
-    return !per_block && r.in_stride == n && r.out_stride == n && ((uint64_t)r.batch * n) % kTileWords == 0;
+    return r.in_stride == n && r.out_stride == n && ((uint64_t)r.batch * n) % kTileWords == 0;
   }
   return r.P >= 1 && r.P <= 8 && r.lo >= 5 && r.lo + r.P <= r.log_n;
 }
@@ -134,7 +135,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
 
 template <class F, bool DESC>
 Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
-  if (!tma_pass_ok(r, !F::kMontgomery)) return {SFNTT_INVALID_ARGUMENT, "pass shape not supported by the TMA engine"};
+  if (!tma_pass_ok(r)) return {SFNTT_INVALID_ARGUMENT, "pass shape not supported by the TMA engine"};
   if (!F::kMontgomery && (r.twist || r.plain)) return {SFNTT_INVALID_ARGUMENT, "M31 passes take no twist"};
   if (r.contiguous) {
     switch (r.P) {
