@@ -47,7 +47,10 @@ typedef enum sfntt_status {
 
 typedef enum sfntt_field {
     SFNTT_M31 = 0,       /* Circle NTT (DCCT) over M31       */
-    SFNTT_BABYBEAR = 1   /* radix-2 NTT over BabyBear        */
+    SFNTT_BABYBEAR = 1,  /* radix-2 NTT over BabyBear        */
+    SFNTT_KOALABEAR = 2  /* radix-2 NTT over KoalaBear, p = 2^31 - 2^24 + 1: planned in the reference
+                            (README.md:20), no implementation there.  Montgomery u32 like BabyBear;
+                            two_adic_generator(k) = 3^((p-1)/2^k), log_n <= 24 */
 } sfntt_field;
 
 /* Algorithm variants of the reference shootout (src/ntt/mod.rs:17-25). */
@@ -117,6 +120,15 @@ int sfntt_bb_coset_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t 
                        uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode,
                        uint32_t *out, uint64_t *gpu_ns);
 
+/* The same coset LDE for either Montgomery field: field = SFNTT_BABYBEAR
+ * (identical to sfntt_bb_coset_lde) or SFNTT_KOALABEAR (no reference
+ * implementation; the BabyBear algorithm with KoalaBear's constants, shift_monty
+ * == 0 selecting two_adic_generator(log_n + added_bits + 1), log_n + added_bits
+ * <= 23). */
+int sfntt_coset_lde(sfntt_ctx *ctx, int field, const uint32_t *in, size_t len, uint32_t log_n,
+                    uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode,
+                    uint32_t *out, uint64_t *gpu_ns);
+
 /* M31 blow-up (no reference counterpart: the composition of the reference's
  * inverse on odds(log_n), zero-pad, forward on odds(log_n + added_bits)). */
 int sfntt_m31_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n,
@@ -136,6 +148,9 @@ int sfntt_inverse_dev(sfntt_ctx *ctx, int field, int variant, uint32_t *d_data, 
 int sfntt_bb_coset_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
                            uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode,
                            void *stream);
+int sfntt_coset_lde_dev(sfntt_ctx *ctx, int field, const uint32_t *d_in, uint32_t *d_out,
+                        uint32_t log_n, uint32_t batch, uint32_t added_bits, uint32_t shift_monty,
+                        int mode, void *stream);
 int sfntt_m31_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
                       uint32_t batch, uint32_t added_bits, void *stream);
 
@@ -162,13 +177,17 @@ int sfntt_layout(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n,
 /* BabyBear::to_monty / from_monty (src/field/babybear.rs:54-65) on device. */
 int sfntt_bb_to_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
 int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *stream);
+/* The same for field = SFNTT_BABYBEAR or SFNTT_KOALABEAR. */
+int sfntt_to_monty_dev(sfntt_ctx *ctx, int field, uint32_t *d_data, size_t len, void *stream);
+int sfntt_from_monty_dev(sfntt_ctx *ctx, int field, uint32_t *d_data, size_t len, void *stream);
 
 /* ---- Uneven batches in one graph launch (no reference counterpart: the
  * north-star batching pattern).  An item is `batch` SoA columns of 2^log_n
- * points of either field, extended by 2^added_bits: BabyBear items are the
+ * points of any field, extended by 2^added_bits: BabyBear items are the
  * coset LDE of CosetLdeBatch::execute (src/lde/mod.rs:43-107, shift_monty 0 =
- * reference shift), M31 items the composition inverse(odds(log_n)) -> zero-pad
- * -> forward(odds(log_n + added_bits)).  Device pointers. */
+ * reference shift), KoalaBear items the same LDE over KoalaBear, M31 items the
+ * composition inverse(odds(log_n)) -> zero-pad -> forward(odds(log_n +
+ * added_bits)).  Device pointers. */
 typedef enum sfntt_plan {
     SFNTT_PLAN_AUTO = 0,           /* tuned plan for the item's key, else the context default */
     SFNTT_PLAN_TMA = 1,            /* persistent TMA engine, per-position strided twiddles */

@@ -13,65 +13,95 @@
 #include <omp.h>
 #endif
 
-/* ===================== BabyBear (src/field/babybear.rs) ================== */
+/* ================ Montgomery fields (src/field/babybear.rs) ============== */
 
-#define BB_P ORC_BB_P
-#define BB_R2 1172168163u        /* babybear.rs:25 R^2 mod p            */
-#define BB_MONTY_CONST 2013265919u /* babybear.rs:29 -p^-1 mod 2^32      */
-#define BB_ONE 268435454u        /* babybear.rs:22 R mod p (Montgomery 1) */
-#define BB_TWO_ADICITY 27u       /* babybear.rs:33                       */
-#define BB_ROOT_MONTY 1476048622u /* babybear.rs:37 (440564289 canonical) */
+/* BabyBear's arithmetic restated over a field descriptor, so that KoalaBear
+ * (p = 2^31 - 2^24 + 1, listed as planned in the reference's README.md:20 and
+ * not implemented there) runs the very code the BabyBear golden vectors pin,
+ * with its own constants. */
+typedef struct {
+    uint32_t p, r2, monty_const, one, two_adicity, root_monty;
+} mfield;
 
-uint32_t orc_bb_monty_reduce(uint64_t t) /* babybear.rs:41-51 */
+static const mfield MF_BB = {
+    ORC_BB_P,
+    1172168163u,  /* babybear.rs:25 R^2 mod p            */
+    2013265919u,  /* babybear.rs:29 -p^-1 mod 2^32       */
+    268435454u,   /* babybear.rs:22 R mod p (Montgomery 1) */
+    27u,          /* babybear.rs:33                      */
+    1476048622u,  /* babybear.rs:37 (440564289 canonical = 31^((p-1)/2^27)) */
+};
+
+/* KoalaBear: p - 1 = 2^24 * 127, generator 3, root 3^((p-1)/2^24) =
+ * 1791270792 canonical (the construction of BabyBear's root from its
+ * generator 31).  R^2, -p^-1 and R are computed from p by the usual
+ * definitions; tests/test_oracle.py recomputes every constant. */
+static const mfield MF_KB = {
+    ORC_KB_P,
+    402124772u,   /* R^2 mod p         */
+    2130706431u,  /* -p^-1 mod 2^32    */
+    33554430u,    /* R mod p           */
+    24u,
+    331895189u,   /* 1791270792 * R mod p */
+};
+
+static uint32_t mf_reduce(const mfield *f, uint64_t t) /* babybear.rs:41-51 */
 {
     uint32_t t_lo = (uint32_t)t;
-    uint32_t m = t_lo * BB_MONTY_CONST;
-    uint64_t mp = (uint64_t)m * BB_P;
+    uint32_t m = t_lo * f->monty_const;
+    uint64_t mp = (uint64_t)m * f->p;
     uint32_t r = (uint32_t)((t + mp) >> 32);
-    return r >= BB_P ? r - BB_P : r;
+    return r >= f->p ? r - f->p : r;
 }
 
-uint32_t orc_bb_to_monty(uint32_t v) { return orc_bb_monty_reduce((uint64_t)v * BB_R2); }
-uint32_t orc_bb_from_monty(uint32_t m) { return orc_bb_monty_reduce((uint64_t)m); }
-
-uint32_t orc_bb_add(uint32_t a, uint32_t b) /* babybear.rs:113-121 */
+static uint32_t mf_to_monty(const mfield *f, uint32_t v) { return mf_reduce(f, (uint64_t)v * f->r2); }
+static uint32_t mf_add(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:113-121 */
 {
     uint32_t s = a + b;
-    return s >= BB_P ? s - BB_P : s;
+    return s >= f->p ? s - f->p : s;
 }
-
-uint32_t orc_bb_sub(uint32_t a, uint32_t b) /* babybear.rs:124-130 */
+static uint32_t mf_sub(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:124-130 */
 {
-    return a >= b ? a - b : BB_P - (b - a);
+    return a >= b ? a - b : f->p - (b - a);
 }
-
-uint32_t orc_bb_mul(uint32_t a, uint32_t b) /* babybear.rs:133-137 */
+static uint32_t mf_mul(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:133-137 */
 {
-    return orc_bb_monty_reduce((uint64_t)a * b);
+    return mf_reduce(f, (uint64_t)a * b);
 }
-
-uint32_t orc_bb_reduce(uint64_t v) /* babybear.rs:140-145 */
+static uint32_t mf_inv(const mfield *f, uint32_t a) /* babybear.rs:147-161, Fermat a^(p-2) */
 {
-    return orc_bb_to_monty((uint32_t)(v % BB_P));
-}
-
-uint32_t orc_bb_inv(uint32_t a) /* babybear.rs:147-161, Fermat a^(p-2) */
-{
-    uint32_t result = BB_ONE, base = a, e = BB_P - 2;
+    uint32_t result = f->one, base = a, e = f->p - 2;
     while (e > 0) {
-        if (e & 1) result = orc_bb_mul(result, base);
-        base = orc_bb_mul(base, base);
+        if (e & 1) result = mf_mul(f, result, base);
+        base = mf_mul(f, base, base);
         e >>= 1;
     }
     return result;
 }
-
-uint32_t orc_bb_two_adic_generator(uint32_t log_n) /* babybear.rs:69-76 */
+static uint32_t mf_two_adic_generator(const mfield *f, uint32_t log_n) /* babybear.rs:69-76 */
 {
-    uint32_t g = BB_ROOT_MONTY;
-    for (uint32_t i = 0; i < BB_TWO_ADICITY - log_n; i++) g = orc_bb_mul(g, g);
+    uint32_t g = f->root_monty;
+    for (uint32_t i = 0; i < f->two_adicity - log_n; i++) g = mf_mul(f, g, g);
     return g;
 }
+
+uint32_t orc_bb_monty_reduce(uint64_t t) { return mf_reduce(&MF_BB, t); }
+uint32_t orc_bb_to_monty(uint32_t v) { return mf_to_monty(&MF_BB, v); }
+uint32_t orc_bb_from_monty(uint32_t m) { return mf_reduce(&MF_BB, (uint64_t)m); }
+uint32_t orc_bb_add(uint32_t a, uint32_t b) { return mf_add(&MF_BB, a, b); }
+uint32_t orc_bb_sub(uint32_t a, uint32_t b) { return mf_sub(&MF_BB, a, b); }
+uint32_t orc_bb_mul(uint32_t a, uint32_t b) { return mf_mul(&MF_BB, a, b); }
+uint32_t orc_bb_reduce(uint64_t v) /* babybear.rs:140-145 */
+{
+    return orc_bb_to_monty((uint32_t)(v % ORC_BB_P));
+}
+uint32_t orc_bb_inv(uint32_t a) { return mf_inv(&MF_BB, a); }
+uint32_t orc_bb_two_adic_generator(uint32_t log_n) { return mf_two_adic_generator(&MF_BB, log_n); }
+
+uint32_t orc_kb_to_monty(uint32_t v) { return mf_to_monty(&MF_KB, v); }
+uint32_t orc_kb_from_monty(uint32_t m) { return mf_reduce(&MF_KB, (uint64_t)m); }
+uint32_t orc_kb_mul(uint32_t a, uint32_t b) { return mf_mul(&MF_KB, a, b); }
+uint32_t orc_kb_two_adic_generator(uint32_t log_n) { return mf_two_adic_generator(&MF_KB, log_n); }
 
 /* ========================= M31 (src/field/m31.rs) ======================== */
 
@@ -184,19 +214,22 @@ static size_t bit_reverse_idx(size_t index, uint32_t log_size) /* m31/twiddles.r
 /* BabyBear::generate_twiddles (babybear.rs:83-97): layer s holds g_{s+1}^j,
  * j < 2^s; generate_inverse_twiddles (babybear/twiddles.rs:13-19) inverts
  * every entry. */
-void orc_bb_twiddles(uint32_t log_n, int inverse, uint32_t *out)
+static void mf_twiddles(const mfield *f, uint32_t log_n, int inverse, uint32_t *out)
 {
     for (uint32_t s = 0; s < log_n; s++) {
         size_t half = (size_t)1 << s;
-        uint32_t g = orc_bb_two_adic_generator(s + 1);
-        uint32_t w = BB_ONE;
+        uint32_t g = mf_two_adic_generator(f, s + 1);
+        uint32_t w = f->one;
         uint32_t *layer = out + (half - 1);
         for (size_t j = 0; j < half; j++) {
-            layer[j] = inverse ? orc_bb_inv(w) : w;
-            w = orc_bb_mul(w, g);
+            layer[j] = inverse ? mf_inv(f, w) : w;
+            w = mf_mul(f, w, g);
         }
     }
 }
+
+void orc_bb_twiddles(uint32_t log_n, int inverse, uint32_t *out) { mf_twiddles(&MF_BB, log_n, inverse, out); }
+void orc_kb_twiddles(uint32_t log_n, int inverse, uint32_t *out) { mf_twiddles(&MF_KB, log_n, inverse, out); }
 
 /* generate_twiddles / generate_itwiddles (m31/twiddles.rs:19-68) on
  * Coset::odds(log_n): layer l holds the x coordinate (y on the last layer)
@@ -220,27 +253,31 @@ void orc_m31_twiddles(uint32_t log_n, int inverse, uint32_t *out)
 
 /* TwiddleCache (src/ntt/twiddle_cache.rs): one cached table per
  * (field, direction, log_n).  Tables are filled before any parallel region. */
-static uint32_t *g_tw_cache[2][2][32];
+enum { TW_BB = 0, TW_M31 = 1, TW_KB = 2 };
+static uint32_t *g_tw_cache[3][2][32];
 
-static const uint32_t *tw_get(int field_m31, int inverse, uint32_t log_n)
+static const uint32_t *tw_get(int field, int inverse, uint32_t log_n)
 {
-    uint32_t **slot = &g_tw_cache[field_m31][inverse][log_n];
+    uint32_t **slot = &g_tw_cache[field][inverse][log_n];
     if (*slot == NULL) {
         size_t n = (size_t)1 << log_n;
         uint32_t *t = (uint32_t *)malloc(n * sizeof(uint32_t));
-        if (field_m31) orc_m31_twiddles(log_n, inverse, t);
+        if (field == TW_M31) orc_m31_twiddles(log_n, inverse, t);
+        else if (field == TW_KB) orc_kb_twiddles(log_n, inverse, t);
         else orc_bb_twiddles(log_n, inverse, t);
         *slot = t;
     }
     return *slot;
 }
 
+static int mf_tw_id(const mfield *f) { return f == &MF_KB ? TW_KB : TW_BB; }
+
 static int is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
 static uint32_t ilog2(size_t n) { uint32_t l = 0; while (((size_t)1 << l) < n) l++; return l; }
 
 /* ====================== BabyBear NTT (cpu_reference.rs) ================== */
 
-static void bb_forward_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *tw)
+static void mf_forward_tw(const mfield *f, uint32_t *data, size_t n, uint32_t log_n, const uint32_t *tw)
 {
     for (int layer = (int)log_n - 1; layer >= 0; layer--) { /* cpu_reference.rs:45-60 */
         size_t half = (size_t)1 << layer, full = half << 1;
@@ -249,14 +286,14 @@ static void bb_forward_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32
             for (size_t j = 0; j < half; j++) {
                 size_t i0 = block * full + j, i1 = i0 + half;
                 uint32_t v0 = data[i0], v1 = data[i1];
-                data[i0] = orc_bb_add(v0, v1);
-                data[i1] = orc_bb_mul(orc_bb_sub(v0, v1), t[j]);
+                data[i0] = mf_add(f, v0, v1);
+                data[i1] = mf_mul(f, mf_sub(f, v0, v1), t[j]);
             }
         }
     }
 }
 
-static void bb_inverse_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32_t *itw,
+static void mf_inverse_tw(const mfield *f, uint32_t *data, size_t n, uint32_t log_n, const uint32_t *itw,
                           int normalize)
 {
     for (uint32_t layer = 0; layer < log_n; layer++) { /* cpu_reference.rs:80-95 */
@@ -265,38 +302,43 @@ static void bb_inverse_tw(uint32_t *data, size_t n, uint32_t log_n, const uint32
         for (size_t block = 0; block < n / full; block++) {
             for (size_t j = 0; j < half; j++) {
                 size_t i0 = block * full + j, i1 = i0 + half;
-                uint32_t tmp = orc_bb_mul(data[i1], t[j]);
+                uint32_t tmp = mf_mul(f, data[i1], t[j]);
                 uint32_t v0 = data[i0];
-                data[i0] = orc_bb_add(v0, tmp);
-                data[i1] = orc_bb_sub(v0, tmp);
+                data[i0] = mf_add(f, v0, tmp);
+                data[i1] = mf_sub(f, v0, tmp);
             }
         }
     }
     if (normalize) { /* cpu_reference.rs:97-101 */
-        uint32_t inv_n = orc_bb_inv(orc_bb_reduce(n));
-        for (size_t i = 0; i < n; i++) data[i] = orc_bb_mul(data[i], inv_n);
+        uint32_t inv_n = mf_inv(f, mf_to_monty(f, (uint32_t)(n % f->p)));
+        for (size_t i = 0; i < n; i++) data[i] = mf_mul(f, data[i], inv_n);
     }
 }
 
-int orc_bb_forward(uint32_t *data, size_t n)
+static int mf_forward(const mfield *f, uint32_t *data, size_t n)
 {
     if (!is_pow2(n)) return 1;
     if (n == 1) return 0;
     uint32_t log_n = ilog2(n);
-    if (log_n > BB_TWO_ADICITY) return 1;
-    bb_forward_tw(data, n, log_n, tw_get(0, 0, log_n));
+    if (log_n > f->two_adicity) return 1;
+    mf_forward_tw(f, data, n, log_n, tw_get(mf_tw_id(f), 0, log_n));
     return 0;
 }
 
-int orc_bb_inverse(uint32_t *data, size_t n)
+static int mf_inverse(const mfield *f, uint32_t *data, size_t n)
 {
     if (!is_pow2(n)) return 1;
     if (n == 1) return 0;
     uint32_t log_n = ilog2(n);
-    if (log_n > BB_TWO_ADICITY) return 1;
-    bb_inverse_tw(data, n, log_n, tw_get(0, 1, log_n), 1);
+    if (log_n > f->two_adicity) return 1;
+    mf_inverse_tw(f, data, n, log_n, tw_get(mf_tw_id(f), 1, log_n), 1);
     return 0;
 }
+
+int orc_bb_forward(uint32_t *data, size_t n) { return mf_forward(&MF_BB, data, n); }
+int orc_bb_inverse(uint32_t *data, size_t n) { return mf_inverse(&MF_BB, data, n); }
+int orc_kb_forward(uint32_t *data, size_t n) { return mf_forward(&MF_KB, data, n); }
+int orc_kb_inverse(uint32_t *data, size_t n) { return mf_inverse(&MF_KB, data, n); }
 
 /* ======================== M31 NTT (m31/cpu_reference.rs) ================= */
 
@@ -343,7 +385,7 @@ int orc_m31_forward(uint32_t *data, size_t n)
     if (n == 1) return 0;
     uint32_t log_n = ilog2(n);
     if (log_n > 30) return 1;
-    m31_forward_tw(data, n, log_n, tw_get(1, 0, log_n));
+    m31_forward_tw(data, n, log_n, tw_get(TW_M31, 0, log_n));
     return 0;
 }
 
@@ -353,7 +395,7 @@ int orc_m31_inverse(uint32_t *data, size_t n)
     if (n == 1) return 0;
     uint32_t log_n = ilog2(n);
     if (log_n > 30) return 1;
-    m31_inverse_tw(data, n, log_n, tw_get(1, 1, log_n));
+    m31_inverse_tw(data, n, log_n, tw_get(TW_M31, 1, log_n));
     return 0;
 }
 
@@ -361,30 +403,47 @@ int orc_m31_inverse(uint32_t *data, size_t n)
 
 static int clamp_threads(int threads) { return threads < 1 ? 1 : threads; }
 
-int orc_bb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+static int mf_forward_batch(const mfield *f, uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
 {
-    if (log_n > BB_TWO_ADICITY) return 1;
+    if (log_n > f->two_adicity) return 1;
     if (log_n == 0) return 0;
     size_t n = (size_t)1 << log_n;
-    const uint32_t *tw = tw_get(0, 0, log_n);
+    const uint32_t *tw = tw_get(mf_tw_id(f), 0, log_n);
     long c;
     (void)threads;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
-    for (c = 0; c < (long)batch; c++) bb_forward_tw(data + (size_t)c * n, n, log_n, tw);
+    for (c = 0; c < (long)batch; c++) mf_forward_tw(f, data + (size_t)c * n, n, log_n, tw);
     return 0;
 }
 
-int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+static int mf_inverse_batch(const mfield *f, uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
 {
-    if (log_n > BB_TWO_ADICITY) return 1;
+    if (log_n > f->two_adicity) return 1;
     if (log_n == 0) return 0;
     size_t n = (size_t)1 << log_n;
-    const uint32_t *itw = tw_get(0, 1, log_n);
+    const uint32_t *itw = tw_get(mf_tw_id(f), 1, log_n);
     long c;
     (void)threads;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
-    for (c = 0; c < (long)batch; c++) bb_inverse_tw(data + (size_t)c * n, n, log_n, itw, 1);
+    for (c = 0; c < (long)batch; c++) mf_inverse_tw(f, data + (size_t)c * n, n, log_n, itw, 1);
     return 0;
+}
+
+int orc_bb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    return mf_forward_batch(&MF_BB, data, log_n, batch, threads);
+}
+int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    return mf_inverse_batch(&MF_BB, data, log_n, batch, threads);
+}
+int orc_kb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    return mf_forward_batch(&MF_KB, data, log_n, batch, threads);
+}
+int orc_kb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads)
+{
+    return mf_inverse_batch(&MF_KB, data, log_n, batch, threads);
 }
 
 /* ========================= Coset LDE (src/lde/mod.rs) ==================== */
@@ -392,35 +451,47 @@ int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int thr
 /* coset_lde_batch_cpu (lde/mod.rs:127-176): per-column inverse, zero-pad
  * copy, coset shift over rows-then-columns with shift =
  * two_adic_generator(log_n_ext + 1) (lde/mod.rs:158), per-column forward. */
-int orc_bb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
-                     uint32_t added_bits, uint32_t shift_monty, int threads)
+static int mf_coset_lde(const mfield *f, const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                        uint32_t added_bits, uint32_t shift_monty, int threads)
 {
     uint32_t log_n_ext = log_n + added_bits;
-    if (log_n_ext + 1 > BB_TWO_ADICITY) return 1;
+    if (log_n_ext + 1 > f->two_adicity) return 1;
     size_t n = (size_t)1 << log_n, n_ext = (size_t)1 << log_n_ext;
-    uint32_t shift = shift_monty ? shift_monty : orc_bb_two_adic_generator(log_n_ext + 1);
-    const uint32_t *itw = log_n ? tw_get(0, 1, log_n) : NULL;
-    const uint32_t *tw = log_n_ext ? tw_get(0, 0, log_n_ext) : NULL;
+    uint32_t shift = shift_monty ? shift_monty : mf_two_adic_generator(f, log_n_ext + 1);
+    const uint32_t *itw = log_n ? tw_get(mf_tw_id(f), 1, log_n) : NULL;
+    const uint32_t *tw = log_n_ext ? tw_get(mf_tw_id(f), 0, log_n_ext) : NULL;
     long c;
     (void)threads;
 
     /* shift powers, shared by every column (the reference recomputes the
      * running power in its row loop; the values are identical) */
     uint32_t *pw = (uint32_t *)malloc(n_ext * sizeof(uint32_t));
-    uint32_t p = BB_ONE;
-    for (size_t i = 0; i < n_ext; i++) { pw[i] = p; p = orc_bb_mul(p, shift); }
+    uint32_t p = f->one;
+    for (size_t i = 0; i < n_ext; i++) { pw[i] = p; p = mf_mul(f, p, shift); }
 
 #pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
     for (c = 0; c < (long)batch; c++) {
         uint32_t *dst = out + (size_t)c * n_ext;
         memcpy(dst, in + (size_t)c * n, n * sizeof(uint32_t));          /* step 1+2 */
-        if (log_n) bb_inverse_tw(dst, n, log_n, itw, 1);
+        if (log_n) mf_inverse_tw(f, dst, n, log_n, itw, 1);
         memset(dst + n, 0, (n_ext - n) * sizeof(uint32_t));
-        for (size_t i = 0; i < n_ext; i++) dst[i] = orc_bb_mul(dst[i], pw[i]); /* step 3 */
-        if (log_n_ext) bb_forward_tw(dst, n_ext, log_n_ext, tw);        /* step 4 */
+        for (size_t i = 0; i < n_ext; i++) dst[i] = mf_mul(f, dst[i], pw[i]); /* step 3 */
+        if (log_n_ext) mf_forward_tw(f, dst, n_ext, log_n_ext, tw);     /* step 4 */
     }
     free(pw);
     return 0;
+}
+
+int orc_bb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                     uint32_t added_bits, uint32_t shift_monty, int threads)
+{
+    return mf_coset_lde(&MF_BB, in, out, log_n, batch, added_bits, shift_monty, threads);
+}
+
+int orc_kb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                     uint32_t added_bits, uint32_t shift_monty, int threads)
+{
+    return mf_coset_lde(&MF_KB, in, out, log_n, batch, added_bits, shift_monty, threads);
 }
 
 int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
@@ -429,8 +500,8 @@ int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batc
     uint32_t log_n_ext = log_n + added_bits;
     if (log_n_ext > 30) return 1;
     size_t n = (size_t)1 << log_n, n_ext = (size_t)1 << log_n_ext;
-    const uint32_t *itw = log_n ? tw_get(1, 1, log_n) : NULL;
-    const uint32_t *tw = log_n_ext ? tw_get(1, 0, log_n_ext) : NULL;
+    const uint32_t *itw = log_n ? tw_get(TW_M31, 1, log_n) : NULL;
+    const uint32_t *tw = log_n_ext ? tw_get(TW_M31, 0, log_n_ext) : NULL;
     long c;
     (void)threads;
 #pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
@@ -452,7 +523,7 @@ uint64_t orc_lcg_fill(uint32_t *out, size_t n, uint64_t seed, uint32_t p, int mo
     for (size_t i = 0; i < n; i++) {
         s = s * 6364136223846793005ull + 1ull;
         uint32_t v = (uint32_t)(s >> 33) % p;
-        out[i] = monty ? orc_bb_to_monty(v) : v;
+        out[i] = monty == 2 ? orc_kb_to_monty(v) : (monty ? orc_bb_to_monty(v) : v);
     }
     return s;
 }

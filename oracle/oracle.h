@@ -19,6 +19,13 @@
  *   src/ntt/babybear/cpu_reference.rs:34-103  GS-DIF forward / CT-DIT inverse
  *   src/lde/mod.rs:116-176            coset_lde_batch_cpu
  *
+ * KoalaBear (p = 2^31 - 2^24 + 1) is listed as planned in the reference's
+ * README.md:20 and not implemented there: the orc_kb_* functions run the
+ * BabyBear code above over KoalaBear's constants (generator 3, primitive
+ * 2^24-th root 3^((p-1)/2^24)).  They are pinned by the same code path's
+ * BabyBear golden vectors and by a direct O(n^2) DFT in the tests, not by
+ * any reference output.
+ *
  * Every function keeps the reference's loop structure (layer -> block -> j)
  * so that it can also serve as the timed CPU baseline.
  */
@@ -34,6 +41,7 @@ extern "C" {
 
 #define ORC_BB_P 2013265921u          /* 0x78000001 */
 #define ORC_M31_P 2147483647u         /* 2^31 - 1   */
+#define ORC_KB_P 2130706433u          /* 0x7F000001: KoalaBear, 2^31 - 2^24 + 1 */
 
 /* ---- BabyBear field (src/field/babybear.rs) ---------------------------- */
 uint32_t orc_bb_monty_reduce(uint64_t t);        /* babybear.rs:41-51 */
@@ -93,9 +101,24 @@ int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
 int orc_bb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
 int orc_bb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
 
+/* ---- KoalaBear (same algorithms and conventions as BabyBear) ----------- */
+uint32_t orc_kb_to_monty(uint32_t v);
+uint32_t orc_kb_from_monty(uint32_t m);
+uint32_t orc_kb_mul(uint32_t a, uint32_t b);
+uint32_t orc_kb_two_adic_generator(uint32_t log_n);  /* Montgomery form */
+void orc_kb_twiddles(uint32_t log_n, int inverse, uint32_t *out);
+int orc_kb_forward(uint32_t *data, size_t n);
+int orc_kb_inverse(uint32_t *data, size_t n);
+int orc_kb_forward_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
+int orc_kb_inverse_batch(uint32_t *data, uint32_t log_n, uint32_t batch, int threads);
+int orc_kb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
+                     uint32_t batch, uint32_t added_bits, uint32_t shift_monty,
+                     int threads);
+
 /* Reference data generator (src/ntt/test_utils.rs:38-46, benches seeds):
- * s = s*6364136223846793005 + 1; v = (s >> 33) % p.  to_monty applied when
- * monty != 0.  Returns the final state. */
+ * s = s*6364136223846793005 + 1; v = (s >> 33) % p.  BabyBear to_monty
+ * applied when monty == 1, KoalaBear's when monty == 2.  Returns the final
+ * state. */
 uint64_t orc_lcg_fill(uint32_t *out, size_t n, uint64_t seed, uint32_t p, int monty);
 
 #ifdef __cplusplus

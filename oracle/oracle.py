@@ -19,6 +19,7 @@ LIB_PATH = HERE / "liboracle.so"
 
 BB_P = 2013265921
 M31_P = 2147483647
+KB_P = 2130706433  # KoalaBear, 2^31 - 2^24 + 1 (no reference implementation)
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _lib = None
@@ -72,6 +73,16 @@ def lib():
             "orc_bb_forward_batch": (i, [_u32p, u32, u32, i]),
             "orc_bb_inverse_batch": (i, [_u32p, u32, u32, i]),
             "orc_lcg_fill": (u64, [_u32p, sz, u64, u32, i]),
+            "orc_kb_to_monty": (u32, [u32]),
+            "orc_kb_from_monty": (u32, [u32]),
+            "orc_kb_mul": (u32, [u32, u32]),
+            "orc_kb_two_adic_generator": (u32, [u32]),
+            "orc_kb_twiddles": (None, [u32, i, _u32p]),
+            "orc_kb_forward": (i, [_u32p, sz]),
+            "orc_kb_inverse": (i, [_u32p, sz]),
+            "orc_kb_forward_batch": (i, [_u32p, u32, u32, i]),
+            "orc_kb_inverse_batch": (i, [_u32p, u32, u32, i]),
+            "orc_kb_coset_lde": (i, [_u32p, _u32p, u32, u32, u32, u32, i]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -104,6 +115,10 @@ def bb_inv(a): return lib().orc_bb_inv(a)
 def bb_reduce(v): return lib().orc_bb_reduce(v)
 def bb_monty_reduce(t): return lib().orc_bb_monty_reduce(t)
 def bb_two_adic_generator(k): return lib().orc_bb_two_adic_generator(k)
+def kb_to_monty(v: int) -> int: return lib().orc_kb_to_monty(v)
+def kb_from_monty(m: int) -> int: return lib().orc_kb_from_monty(m)
+def kb_mul(a, b): return lib().orc_kb_mul(a, b)
+def kb_two_adic_generator(k): return lib().orc_kb_two_adic_generator(k)
 def m31_add(a, b): return lib().orc_m31_add(a, b)
 def m31_sub(a, b): return lib().orc_m31_sub(a, b)
 def m31_mul(a, b): return lib().orc_m31_mul(a, b)
@@ -126,6 +141,12 @@ def bb_twiddles(log_n: int, inverse: bool = False) -> np.ndarray:
     return out[: (1 << log_n) - 1]
 
 
+def kb_twiddles(log_n: int, inverse: bool = False) -> np.ndarray:
+    out = np.zeros(max((1 << log_n) - 1, 1), dtype=np.uint32)
+    lib().orc_kb_twiddles(log_n, int(inverse), _ptr(out))
+    return out[: (1 << log_n) - 1]
+
+
 def m31_twiddles(log_n: int, inverse: bool = False) -> np.ndarray:
     out = np.zeros(max((1 << log_n) - 1, 1), dtype=np.uint32)
     lib().orc_m31_twiddles(log_n, int(inverse), _ptr(out))
@@ -142,36 +163,56 @@ def _one(fn, data) -> np.ndarray:
 
 def bb_forward(data) -> np.ndarray: return _one(lib().orc_bb_forward, data)
 def bb_inverse(data) -> np.ndarray: return _one(lib().orc_bb_inverse, data)
+def kb_forward(data) -> np.ndarray: return _one(lib().orc_kb_forward, data)
+def kb_inverse(data) -> np.ndarray: return _one(lib().orc_kb_inverse, data)
 def m31_forward(data) -> np.ndarray: return _one(lib().orc_m31_forward, data)
 def m31_inverse(data) -> np.ndarray: return _one(lib().orc_m31_inverse, data)
 
 
-def bb_forward_batch(data, log_n: int, batch: int, threads: int = 1) -> np.ndarray:
+def _batch(fn, data, log_n: int, batch: int, threads: int) -> np.ndarray:
     a = _arr(data).copy()
     assert a.size == batch << log_n
-    if lib().orc_bb_forward_batch(_ptr(a), log_n, batch, threads) != 0:
+    if fn(_ptr(a), log_n, batch, threads) != 0:
         raise InvalidSize(a.size)
     return a
+
+
+def bb_forward_batch(data, log_n: int, batch: int, threads: int = 1) -> np.ndarray:
+    return _batch(lib().orc_bb_forward_batch, data, log_n, batch, threads)
 
 
 def bb_inverse_batch(data, log_n: int, batch: int, threads: int = 1) -> np.ndarray:
-    a = _arr(data).copy()
-    assert a.size == batch << log_n
-    if lib().orc_bb_inverse_batch(_ptr(a), log_n, batch, threads) != 0:
-        raise InvalidSize(a.size)
-    return a
+    return _batch(lib().orc_bb_inverse_batch, data, log_n, batch, threads)
 
 
-def bb_coset_lde(data, log_n: int, batch: int, added_bits: int, shift_monty: int = 0,
-                 threads: int = 1) -> np.ndarray:
+def kb_forward_batch(data, log_n: int, batch: int, threads: int = 1) -> np.ndarray:
+    return _batch(lib().orc_kb_forward_batch, data, log_n, batch, threads)
+
+
+def kb_inverse_batch(data, log_n: int, batch: int, threads: int = 1) -> np.ndarray:
+    return _batch(lib().orc_kb_inverse_batch, data, log_n, batch, threads)
+
+
+def _coset_lde(fn, data, log_n, batch, added_bits, shift_monty, threads) -> np.ndarray:
     a = _arr(data)
     if a.size != batch << log_n:
         raise InvalidSize(a.size)
     out = np.empty(batch << (log_n + added_bits), dtype=np.uint32)
-    if lib().orc_bb_coset_lde(_ptr(a), _ptr(out), log_n, batch, added_bits, shift_monty,
-                              threads) != 0:
+    if fn(_ptr(a), _ptr(out), log_n, batch, added_bits, shift_monty, threads) != 0:
         raise InvalidSize(a.size)
     return out
+
+
+def bb_coset_lde(data, log_n: int, batch: int, added_bits: int, shift_monty: int = 0,
+                 threads: int = 1) -> np.ndarray:
+    return _coset_lde(lib().orc_bb_coset_lde, data, log_n, batch, added_bits, shift_monty, threads)
+
+
+def kb_coset_lde(data, log_n: int, batch: int, added_bits: int, shift_monty: int = 0,
+                 threads: int = 1) -> np.ndarray:
+    """KoalaBear coset LDE: the BabyBear algorithm over KoalaBear (Montgomery
+    u32 in and out; shift_monty 0 = two_adic_generator(log_n + added_bits + 1))."""
+    return _coset_lde(lib().orc_kb_coset_lde, data, log_n, batch, added_bits, shift_monty, threads)
 
 
 def m31_lde(data, log_n: int, batch: int, added_bits: int, threads: int = 1) -> np.ndarray:
@@ -185,10 +226,11 @@ def m31_lde(data, log_n: int, batch: int, added_bits: int, threads: int = 1) -> 
 
 
 def lcg(n: int, seed: int, p: int, monty: bool = False) -> np.ndarray:
-    """The reference LCG (src/ntt/test_utils.rs:38-46): values (s>>33) % p."""
+    """The reference LCG (src/ntt/test_utils.rs:38-46): values (s>>33) % p,
+    in p's Montgomery form when `monty` (BabyBear or KoalaBear by p)."""
     out = np.empty(n, dtype=np.uint32)
     if n:
-        lib().orc_lcg_fill(_ptr(out), n, seed, p, int(monty))
+        lib().orc_lcg_fill(_ptr(out), n, seed, p, (2 if p == KB_P else 1) if monty else 0)
     return out
 
 

@@ -39,7 +39,13 @@ struct BabyBear {
   uint32_t v;  // Montgomery form
   static constexpr int kField = SFNTT_BABYBEAR;
 };
-static_assert(sizeof(M31) == 4 && sizeof(BabyBear) == 4, "field elements are one u32");
+// KoalaBear (p = 2^31 - 2^24 + 1): planned in the reference (README.md:20), no
+// type there; Montgomery form like BabyBear.
+struct KoalaBear {
+  uint32_t v;  // Montgomery form
+  static constexpr int kField = SFNTT_KOALABEAR;
+};
+static_assert(sizeof(M31) == 4 && sizeof(BabyBear) == 4 && sizeof(KoalaBear) == 4, "field elements are one u32");
 
 enum class Variant : int { Best = SFNTT_BEST, CtDitR2 = 1, CtGsR2 = 2, StockhamR2 = 3, CtGsR4 = 4 };
 
@@ -193,13 +199,13 @@ class CudaBackend final : public NttBackend<F> {
 
  private:
   static constexpr std::string_view name_of() {
-    constexpr bool bb = F::kField == SFNTT_BABYBEAR;
+    constexpr bool bb = F::kField == SFNTT_BABYBEAR, kb = F::kField == SFNTT_KOALABEAR;
     switch (V) {
-      case Variant::CtDitR2: return bb ? "bb-cuda-ct-dit-r2" : "cuda-ct-dit-r2";
-      case Variant::CtGsR2: return bb ? "bb-cuda-r2" : "cuda-ct-gs-r2";
-      case Variant::StockhamR2: return bb ? "bb-cuda-stockham-r2" : "cuda-stockham-r2";
-      case Variant::CtGsR4: return bb ? "bb-cuda-ct-gs-r4" : "cuda-ct-gs-r4";
-      default: return bb ? "bb-cuda" : "cuda";
+      case Variant::CtDitR2: return bb ? "bb-cuda-ct-dit-r2" : kb ? "kb-cuda-ct-dit-r2" : "cuda-ct-dit-r2";
+      case Variant::CtGsR2: return bb ? "bb-cuda-r2" : kb ? "kb-cuda-r2" : "cuda-ct-gs-r2";
+      case Variant::StockhamR2: return bb ? "bb-cuda-stockham-r2" : kb ? "kb-cuda-stockham-r2" : "cuda-stockham-r2";
+      case Variant::CtGsR4: return bb ? "bb-cuda-ct-gs-r4" : kb ? "kb-cuda-ct-gs-r4" : "cuda-ct-gs-r4";
+      default: return bb ? "bb-cuda" : kb ? "kb-cuda" : "cuda";
     }
   }
   static constexpr std::string_view kName = name_of();
@@ -236,6 +242,11 @@ using BbCudaCtDitR2 = CudaBackend<BabyBear, Variant::CtDitR2>;
 using BbBatchNtt = CudaBackend<BabyBear, Variant::CtGsR2>;
 using BbCudaStockhamR2 = CudaBackend<BabyBear, Variant::StockhamR2>;
 using BbCudaCtGsR4 = CudaBackend<BabyBear, Variant::CtGsR4>;
+// KoalaBear backends: the BabyBear variants over KoalaBear.
+using KbCudaCtDitR2 = CudaBackend<KoalaBear, Variant::CtDitR2>;
+using KbBatchNtt = CudaBackend<KoalaBear, Variant::CtGsR2>;
+using KbCudaStockhamR2 = CudaBackend<KoalaBear, Variant::StockhamR2>;
+using KbCudaCtGsR4 = CudaBackend<KoalaBear, Variant::CtGsR4>;
 // The reference's type names (src/ntt/m31/*, src/ntt/babybear/*, src/ntt/metal_r2.rs:337-340).
 using MetalCtDitR2 = CudaCtDitR2;
 using MetalCtGsR2 = CudaCtGsR2;
@@ -253,16 +264,18 @@ struct LdeResult {
 };
 
 // CosetLdeBatch (src/lde/mod.rs:15-107): iDFT -> x n^-1 -> zero-pad ->
-// x shift^i -> DFT over batch_size BabyBear columns.
+// x shift^i -> DFT over batch_size BabyBear columns (KbCosetLdeBatch: the
+// same over KoalaBear).
 // natural = true: natural-order input evaluations and output rows (Plonky3's
 // coset_lde_batch convention) instead of the reference's bit-reversed ones.
-class CosetLdeBatch {
+template <class F>
+class BasicCosetLdeBatch {
  public:
-  explicit CosetLdeBatch(Context ctx = Context(), bool fused = true, bool natural = false)
+  explicit BasicCosetLdeBatch(Context ctx = Context(), bool fused = true, bool natural = false)
       : ctx_(std::move(ctx)),
         mode_((fused ? SFNTT_LDE_FUSED : SFNTT_LDE_UNFUSED) | (natural ? SFNTT_LDE_NATURAL : 0)) {}
-  static CosetLdeBatch create(const std::string& /*shader_dir*/ = {}, int device = 0) {
-    return CosetLdeBatch(Context(device));
+  static BasicCosetLdeBatch create(const std::string& /*shader_dir*/ = {}, int device = 0) {
+    return BasicCosetLdeBatch(Context(device));
   }
   // shift_monty = 0: the reference shift two_adic_generator(log_n + added_bits + 1).
   LdeResult execute(std::span<const uint32_t> input, size_t log_n, size_t batch_size, size_t added_bits,
@@ -270,16 +283,17 @@ class CosetLdeBatch {
     LdeResult r;
     r.data.resize(batch_size << (log_n + added_bits));
     detail::check(ctx_.handle(),
-                  sfntt_bb_coset_lde(ctx_.handle(), input.data(), input.size(), (uint32_t)log_n, (uint32_t)batch_size,
-                                     (uint32_t)added_bits, shift_monty, mode_, r.data.data(), &r.total_ns),
+                  sfntt_coset_lde(ctx_.handle(), F::kField, input.data(), input.size(), (uint32_t)log_n,
+                                  (uint32_t)batch_size, (uint32_t)added_bits, shift_monty, mode_, r.data.data(),
+                                  &r.total_ns),
                   input.size());
     return r;
   }
   void execute_dev(const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch_size, uint32_t added_bits,
                    uint32_t shift_monty = 0, void* stream = nullptr) const {
     detail::check(ctx_.handle(),
-                  sfntt_bb_coset_lde_dev(ctx_.handle(), d_in, d_out, log_n, batch_size, added_bits, shift_monty, mode_,
-                                         stream),
+                  sfntt_coset_lde_dev(ctx_.handle(), F::kField, d_in, d_out, log_n, batch_size, added_bits,
+                                      shift_monty, mode_, stream),
                   (size_t)batch_size << log_n);
   }
   std::string device_info() const { return ctx_.device_info(); }
@@ -288,6 +302,8 @@ class CosetLdeBatch {
   Context ctx_;
   int mode_;
 };
+using CosetLdeBatch = BasicCosetLdeBatch<BabyBear>;
+using KbCosetLdeBatch = BasicCosetLdeBatch<KoalaBear>;
 
 // M31 blow-up: inverse on odds(log n) -> zero-pad -> forward on
 // odds(log n + added_bits).  No reference counterpart; that composition of

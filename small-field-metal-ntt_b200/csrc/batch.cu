@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "context.hpp"
+#include "host_field.hpp"
 
 struct sfntt_graph {
   int device = 0;
@@ -58,13 +59,14 @@ uint32_t pow2_ceil(uint32_t x) {
 
 std::string key_of(const sfntt_lde_item& it) {
   char buf[96];
-  std::snprintf(buf, sizeof buf, "%s/%u/%u/%u", it.field == SFNTT_BABYBEAR ? "bb" : "m31", it.log_n,
+  const char* tag = it.field == SFNTT_BABYBEAR ? "bb" : (it.field == SFNTT_KOALABEAR ? "kb" : "m31");
+  std::snprintf(buf, sizeof buf, "%s/%u/%u/%u", tag, it.log_n,
                 pow2_ceil(it.batch ? it.batch : 1), it.added_bits);
   return buf;
 }
 
 Status check_item(const sfntt_lde_item& it) {
-  if (it.field != SFNTT_BABYBEAR && it.field != SFNTT_M31) return {SFNTT_INVALID_ARGUMENT, "item: unknown field"};
+  if (!valid_field(it.field)) return {SFNTT_INVALID_ARGUMENT, "item: unknown field"};
   if (it.batch && (!it.d_in || !it.d_out)) return {SFNTT_INVALID_ARGUMENT, "item: null buffer"};
   return {};
 }
@@ -84,9 +86,9 @@ Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
   ctx->no_tma = k.no_tma;
   ctx->ntt_plain = k.ntt_plain;
   ctx->lde_plain = k.lde_plain;
-  Status st = it.field == SFNTT_BABYBEAR
-                  ? bb_lde_dev(ctx, it.d_in, it.d_out, it.log_n, it.batch, it.added_bits, it.shift_monty,
-                               SFNTT_LDE_FUSED, s)
+  Status st = is_monty(it.field)
+                  ? monty_lde_dev(ctx, it.field, it.d_in, it.d_out, it.log_n, it.batch, it.added_bits,
+                                  it.shift_monty, SFNTT_LDE_FUSED, s)
                   : m31_lde_dev(ctx, it.d_in, it.d_out, it.log_n, it.batch, it.added_bits, s);
   ctx->no_tma = saved.no_tma;
   ctx->ntt_plain = saved.ntt_plain;
@@ -98,15 +100,17 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
   SFNTT_TRY(check_item(it));
   const uint2* t = nullptr;
   const uint32_t ext = it.log_n + it.added_bits;
-  if (it.field == SFNTT_BABYBEAR) {
-    if (ext + 1 > 27) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
-    if (it.log_n) SFNTT_TRY(bb_twiddles(ctx, true, it.log_n, s, &t));
-    if (ext) SFNTT_TRY(bb_twiddles(ctx, false, ext, s, &t));
-    if (it.added_bits <= 4) SFNTT_TRY(bb_lde_table(ctx, it.log_n, it.added_bits, it.shift_monty, 0, s, &t));
-    SFNTT_TRY(bb_lde_table(ctx, it.log_n, it.added_bits, it.shift_monty, 1, s, &t));
+  if (is_monty(it.field)) {
+    const int f = it.field;
+    const uint32_t adicity = host::monty_field(f).two_adicity;
+    if (ext + 1 > adicity) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(adicity - 1)};
+    if (it.log_n) SFNTT_TRY(monty_twiddles(ctx, f, true, it.log_n, s, &t));
+    if (ext) SFNTT_TRY(monty_twiddles(ctx, f, false, ext, s, &t));
+    if (it.added_bits <= 4) SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 0, s, &t));
+    SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 1, s, &t));
     if (it.log_n >= 13) {
-      SFNTT_TRY(bb_twist_table(ctx, it.log_n - 8, 8, true, s, &t));
-      SFNTT_TRY(bb_twist_table(ctx, it.log_n - 8, 8, false, s, &t));
+      SFNTT_TRY(monty_twist_table(ctx, f, it.log_n - 8, 8, true, s, &t));
+      SFNTT_TRY(monty_twist_table(ctx, f, it.log_n - 8, 8, false, s, &t));
     }
     // strided-pass twists of the four-step plain-NTT plans inside [0, log_n - 8)
     for (uint32_t top : {it.log_n, ext}) {
@@ -114,8 +118,8 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
       if (lo > 12) {
         const uint32_t s_cnt = (lo - 12 + 7) / 8, c = lo - 8 * s_cnt;
         for (uint32_t i = 0; i < s_cnt; ++i) {
-          SFNTT_TRY(bb_twist_table(ctx, c + 8 * i, 8, true, s, &t));
-          SFNTT_TRY(bb_twist_table(ctx, c + 8 * i, 8, false, s, &t));
+          SFNTT_TRY(monty_twist_table(ctx, f, c + 8 * i, 8, true, s, &t));
+          SFNTT_TRY(monty_twist_table(ctx, f, c + 8 * i, 8, false, s, &t));
         }
       }
     }

@@ -47,13 +47,15 @@ bool is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
 uint32_t ilog2(size_t n) { uint32_t l = 0; while (((size_t)1 << l) < n) ++l; return l; }
 
 Status check_field(int field) {
-  if (field != SFNTT_M31 && field != SFNTT_BABYBEAR) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
+  if (!sfntt::valid_field(field)) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
   return {};
 }
 
 Status check_log(int field, uint32_t log_n) {
-  if (field == SFNTT_BABYBEAR && log_n > sfntt::host::BB_TWO_ADICITY)
-    return {SFNTT_INVALID_SIZE, "BabyBear log_n exceeds two-adicity 27"};
+  if (sfntt::is_monty(field) && log_n > sfntt::host::monty_field(field).two_adicity) {
+    const sfntt::host::MontyField& f = sfntt::host::monty_field(field);
+    return {SFNTT_INVALID_SIZE, std::string(f.name) + " log_n exceeds two-adicity " + std::to_string(f.two_adicity)};
+  }
   if (field == SFNTT_M31 && log_n > 30) return {SFNTT_INVALID_SIZE, "M31 log_n > 30"};  // metal_ct_gs_r4.rs:70-72
   return {};
 }
@@ -170,8 +172,8 @@ Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out
       SFNTT_CU(cudaEventRecord(slot[k].uploaded, up));
       SFNTT_CU(cudaStreamWaitEvent(comp, slot[k].uploaded, 0));
       SFNTT_CU(cudaEventRecord(t0[c], comp));
-      if (field == SFNTT_BABYBEAR)
-        SFNTT_TRY(sfntt::bb_lde_dev(ctx, din[k], dout[k], log_n, cols, added_bits, shift_monty, mode, comp));
+      if (sfntt::is_monty(field))
+        SFNTT_TRY(sfntt::monty_lde_dev(ctx, field, din[k], dout[k], log_n, cols, added_bits, shift_monty, mode, comp));
       else
         SFNTT_TRY(sfntt::m31_lde_dev(ctx, din[k], dout[k], log_n, cols, added_bits, comp));
       SFNTT_CU(cudaEventRecord(t1[c], comp));
@@ -211,8 +213,10 @@ int api_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, uint32_t 
   if (ns) *ns = 0;
   Status s;
   const uint32_t log_ext = log_n + added_bits;
-  if (field == SFNTT_BABYBEAR && log_ext + 1 > sfntt::host::BB_TWO_ADICITY)
-    s = {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
+  s = check_field(field);
+  if (s.ok() && sfntt::is_monty(field) && log_ext + 1 > sfntt::host::monty_field(field).two_adicity)
+    s = {SFNTT_INVALID_SIZE,
+         "log_n + added_bits must be <= " + std::to_string(sfntt::host::monty_field(field).two_adicity - 1)};
   if (field == SFNTT_M31 && log_ext > 30) s = {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (s.ok() && len != ((size_t)batch << log_n))  // src/lde/mod.rs:54-56
     s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != batch << log_n"};
@@ -262,7 +266,8 @@ void sfntt_ctx_destroy(sfntt_ctx* ctx) {
   {
     DeviceGuard dg(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (auto& b : ctx->bb_tw) b.release();
+    for (auto& f : ctx->monty_tw)
+      for (auto& b : f) b.release();
     for (auto& m : ctx->m31_tw)
       for (auto& kv : m) kv.second.release();
     for (auto& kv : ctx->lde_tabs) kv.second.release();
@@ -365,6 +370,12 @@ int sfntt_bb_coset_lde(sfntt_ctx* ctx, const uint32_t* in, size_t len, uint32_t 
   return api_lde(ctx, SFNTT_BABYBEAR, in, len, log_n, batch, added_bits, shift_monty, mode, out, gpu_ns);
 }
 
+int sfntt_coset_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
+                    uint32_t added_bits, uint32_t shift_monty, int mode, uint32_t* out, uint64_t* gpu_ns) {
+  if (field == SFNTT_M31) return finish(ctx, {SFNTT_INVALID_ARGUMENT, "coset LDE needs BabyBear or KoalaBear"});
+  return api_lde(ctx, field, in, len, log_n, batch, added_bits, shift_monty, mode, out, gpu_ns);
+}
+
 int sfntt_m31_lde(sfntt_ctx* ctx, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
                   uint32_t added_bits, uint32_t* out, uint64_t* gpu_ns) {
   return api_lde(ctx, SFNTT_M31, in, len, log_n, batch, added_bits, 0, SFNTT_LDE_FUSED, out, gpu_ns);
@@ -379,8 +390,8 @@ int sfntt_prepare(sfntt_ctx* ctx, int field, uint32_t log_n) {
   if (s.ok() && log_n > 0) {
     const uint2* tw;
     for (int inv = 0; inv < 2 && s.ok(); ++inv)
-      s = field == SFNTT_BABYBEAR ? sfntt::bb_twiddles(ctx, inv, log_n, ctx->stream, &tw)
-                                  : sfntt::m31_twiddles(ctx, inv, log_n, ctx->stream, &tw);
+      s = sfntt::is_monty(field) ? sfntt::monty_twiddles(ctx, field, inv, log_n, ctx->stream, &tw)
+                                 : sfntt::m31_twiddles(ctx, inv, log_n, ctx->stream, &tw);
   }
   return finish(ctx, s);
 }
@@ -390,14 +401,15 @@ int sfntt_prepare_lde(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
   Status s = check_field(field);
-  if (s.ok()) s = check_log(field, log_n + added_bits + (field == SFNTT_BABYBEAR ? 1 : 0));
+  if (s.ok()) s = check_log(field, log_n + added_bits + (sfntt::is_monty(field) ? 1 : 0));
   if (s.ok()) {
     const uint2* tw;
-    if (field == SFNTT_BABYBEAR) {
-      if (log_n) s = sfntt::bb_twiddles(ctx, true, log_n, ctx->stream, &tw);
-      if (s.ok()) s = sfntt::bb_twiddles(ctx, false, log_n + added_bits, ctx->stream, &tw);
-      if (s.ok() && added_bits <= 4) s = sfntt::bb_lde_table(ctx, log_n, added_bits, shift_monty, 0, ctx->stream, &tw);
-      if (s.ok()) s = sfntt::bb_lde_table(ctx, log_n, added_bits, shift_monty, 1, ctx->stream, &tw);
+    if (sfntt::is_monty(field)) {
+      cudaStream_t st = ctx->stream;
+      if (log_n) s = sfntt::monty_twiddles(ctx, field, true, log_n, st, &tw);
+      if (s.ok()) s = sfntt::monty_twiddles(ctx, field, false, log_n + added_bits, st, &tw);
+      if (s.ok() && added_bits <= 4) s = sfntt::monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 0, st, &tw);
+      if (s.ok()) s = sfntt::monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 1, st, &tw);
     } else {
       if (log_n) s = sfntt::m31_twiddles(ctx, true, log_n, ctx->stream, &tw);
       if (s.ok() && log_n) s = sfntt::m31_twiddles(ctx, false, log_n + added_bits, ctx->stream, &tw);
@@ -438,7 +450,21 @@ int sfntt_bb_coset_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out
   Status s;
   if (batch && (!d_in || !d_out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
   if (s.ok())
-    s = sfntt::bb_lde_dev(ctx, d_in, d_out, log_n, batch, added_bits, shift_monty, mode, (cudaStream_t)stream);
+    s = sfntt::monty_lde_dev(ctx, SFNTT_BABYBEAR, d_in, d_out, log_n, batch, added_bits, shift_monty, mode,
+                             (cudaStream_t)stream);
+  return finish(ctx, s);
+}
+
+int sfntt_coset_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n,
+                        uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  Status s;
+  if (batch && (!d_in || !d_out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  if (s.ok())
+    s = sfntt::monty_lde_dev(ctx, field, d_in, d_out, log_n, batch, added_bits, shift_monty, mode,
+                             (cudaStream_t)stream);
   return finish(ctx, s);
 }
 
@@ -494,14 +520,28 @@ int sfntt_bb_to_monty_dev(sfntt_ctx* ctx, uint32_t* d, size_t len, void* stream)
   if (!ctx) return SFNTT_INVALID_ARGUMENT;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
-  return finish(ctx, sfntt::bb_monty_dev(ctx, true, d, len, (cudaStream_t)stream));
+  return finish(ctx, sfntt::monty_convert_dev(ctx, SFNTT_BABYBEAR, true, d, len, (cudaStream_t)stream));
 }
 
 int sfntt_bb_from_monty_dev(sfntt_ctx* ctx, uint32_t* d, size_t len, void* stream) {
   if (!ctx) return SFNTT_INVALID_ARGUMENT;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
-  return finish(ctx, sfntt::bb_monty_dev(ctx, false, d, len, (cudaStream_t)stream));
+  return finish(ctx, sfntt::monty_convert_dev(ctx, SFNTT_BABYBEAR, false, d, len, (cudaStream_t)stream));
+}
+
+int sfntt_to_monty_dev(sfntt_ctx* ctx, int field, uint32_t* d, size_t len, void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::monty_convert_dev(ctx, field, true, d, len, (cudaStream_t)stream));
+}
+
+int sfntt_from_monty_dev(sfntt_ctx* ctx, int field, uint32_t* d, size_t len, void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::monty_convert_dev(ctx, field, false, d, len, (cudaStream_t)stream));
 }
 
 int sfntt_host_alloc(sfntt_ctx* ctx, size_t bytes, void** out) {

@@ -95,13 +95,14 @@ struct sfntt_ctx {
   int sm_count = 0;
   std::atomic<uint64_t> launches{0};
 
-  // Twiddle tables: BabyBear per-layer Shoup pairs (layer s at 2^s - 1),
-  // shared by every n <= 2^bb_log[dir]; M31 per log_n (layer l at n - n/2^l).
-  sfntt::DevBuf bb_tw[2];
-  uint32_t bb_log[2] = {0, 0};
+  // Twiddle tables: BabyBear / KoalaBear per-layer Shoup pairs (layer s at
+  // 2^s - 1), shared by every n <= 2^monty_log[field slot][dir]; M31 per log_n
+  // (layer l at n - n/2^l).
+  sfntt::DevBuf monty_tw[2][2];
+  uint32_t monty_log[2][2] = {{0, 0}, {0, 0}};
   std::map<uint32_t, sfntt::DevBuf> m31_tw[2];
-  // LDE multiplier tables keyed by (log_n, added_bits, shift, kind)
-  std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, sfntt::DevBuf> lde_tabs;
+  // LDE multiplier and twist tables keyed by (field, log_n, added_bits, shift, kind)
+  std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, int>, sfntt::DevBuf> lde_tabs;
 
   // staging for host-memory calls
   sfntt::DevBuf buf_in, buf_out, buf_aux;
@@ -127,25 +128,34 @@ struct sfntt_ctx {
 
 namespace sfntt {
 
+// Montgomery-form fields (BabyBear, KoalaBear) share every kernel family;
+// monty_slot indexes their per-field caches.
+inline bool is_monty(int field) { return field == SFNTT_BABYBEAR || field == SFNTT_KOALABEAR; }
+inline bool valid_field(int field) { return field == SFNTT_M31 || is_monty(field); }
+inline int monty_slot(int field) { return field == SFNTT_KOALABEAR ? 1 : 0; }
+
 // Table accessors (twiddles.cu).  All generate on a miss (allocating) and
-// refuse to do so while `stream` is capturing.
-Status bb_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
+// refuse to do so while `stream` is capturing.  `field` is BabyBear or
+// KoalaBear for the monty_* tables.
+Status monty_twiddles(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, cudaStream_t stream,
+                      const uint2** out);
 Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
 // kind 0: fused LDE multipliers M_q[i] = n^-1 (shift g^{rev(q)})^i, q < 2^added, i < n
 // kind 1: plain shift powers shift^i, i < n_ext (unfused path)
-Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty, int kind,
-                    cudaStream_t stream, const uint2** out);
+Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
+                       int kind, cudaStream_t stream, const uint2** out);
 
-// Twist of a strided BabyBear pass over layers [lo, lo + P), indexed by
-// column position mod 2^(lo+P) (cached like the LDE tables).
-Status bb_twist_table(sfntt_ctx* ctx, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream, const uint2** out);
+// Twist of a strided BabyBear / KoalaBear pass over layers [lo, lo + P),
+// indexed by column position mod 2^(lo+P) (cached like the LDE tables).
+Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream,
+                         const uint2** out);
 
 // Kernel drivers (ntt.cu / lde.cu / elementwise.cu)
 Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d_data, uint32_t log_n,
                uint32_t batch, cudaStream_t stream);
 // Layers [a, b) of a 2^log_n network on `batch` columns (first pass in -> out,
 // later passes in place); scale_w != 0 multiplies the final outputs.
-// edge_twist (BabyBear, TMA engine only): a four-step twist applied to the
+// edge_twist (BabyBear / KoalaBear, TMA engine only): a four-step twist applied to the
 // inputs of a forward range or the outputs of an inverse range, indexed by
 // column position & edge_mask -- the boundary with an adjacent strided pass
 // run by another kernel.
@@ -156,8 +166,9 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
 Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in, uint32_t* d_out,
                    uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize,
                    cudaStream_t stream);
-Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
-                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
+// Coset LDE over BabyBear or KoalaBear (lde.cu).
+Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n,
+                     uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
                    uint32_t added_bits, cudaStream_t stream);
 // n^-1 mod p, canonical (ntt.cu).
@@ -173,11 +184,11 @@ Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
 Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
 Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uint32_t* b, uint32_t* out,
                          size_t n, cudaStream_t stream);
-Status bb_monty_dev(sfntt_ctx* ctx, bool to_monty, uint32_t* d, size_t n, cudaStream_t stream);
+Status monty_convert_dev(sfntt_ctx* ctx, int field, bool to_monty, uint32_t* d, size_t n, cudaStream_t stream);
 Status scale_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint64_t n, uint32_t w_canonical, cudaStream_t stream);
 Status zero_pad_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t log_n, uint32_t batch,
                     uint32_t added_bits, cudaStream_t stream);
-Status mul_table_dev(sfntt_ctx* ctx, uint32_t* d, uint32_t log_n_ext, uint32_t batch, const uint2* tab,
+Status mul_table_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint32_t log_n_ext, uint32_t batch, const uint2* tab,
                      cudaStream_t stream);
 
 inline void count_launch(sfntt_ctx* ctx, uint64_t n = 1) { ctx->launches.fetch_add(n, std::memory_order_relaxed); }

@@ -4,6 +4,8 @@
 #pragma once
 #include <cstdint>
 
+#include "../../include/sfntt.h"
+
 namespace sfntt {
 namespace host {
 
@@ -33,6 +35,36 @@ inline uint32_t bb_from_monty(uint32_t W) { return mulmod(W, invmod((uint32_t)((
 
 // Canonical two_adic_generator(k) (src/field/babybear.rs:69-76).
 inline uint32_t bb_two_adic_generator(uint32_t k) { return powmod(BB_ROOT, 1ull << (BB_TWO_ADICITY - k), BB_P); }
+
+// KoalaBear, p = 2^31 - 2^24 + 1 (planned in the reference, README.md:20):
+// p - 1 = 2^24 * 127, smallest multiplicative generator 3, and the primitive
+// 2^24-th root 3^((p-1)/2^24) -- the same construction as BabyBear's root,
+// which is 31^((p-1)/2^27) for its generator 31.
+constexpr uint32_t KB_P = 0x7F000001u;
+constexpr uint32_t KB_TWO_ADICITY = 24;
+constexpr uint32_t KB_ROOT = 1791270792u;
+
+// The two Montgomery-form (R = 2^32) two-adic fields behind one descriptor.
+struct MontyField {
+  uint32_t p;
+  uint32_t two_adicity;
+  uint32_t root;       // canonical primitive 2^two_adicity-th root of unity
+  uint32_t generator;  // multiplicative generator (the Plonky3-style coset shift)
+  const char* name;
+};
+constexpr MontyField kBabyBear{BB_P, BB_TWO_ADICITY, BB_ROOT, 31u, "BabyBear"};
+constexpr MontyField kKoalaBear{KB_P, KB_TWO_ADICITY, KB_ROOT, 3u, "KoalaBear"};
+inline const MontyField& monty_field(int field) { return field == SFNTT_KOALABEAR ? kKoalaBear : kBabyBear; }
+
+inline uint32_t field_p(int field) { return field == SFNTT_M31 ? M31_P : monty_field(field).p; }
+
+inline uint32_t to_monty(const MontyField& f, uint32_t w) { return (uint32_t)(((uint64_t)w << 32) % f.p); }
+inline uint32_t from_monty(const MontyField& f, uint32_t W) {
+  return mulmod(W, invmod((uint32_t)((1ull << 32) % f.p), f.p), f.p);
+}
+inline uint32_t two_adic_generator(const MontyField& f, uint32_t k) {
+  return powmod(f.root, 1ull << (f.two_adicity - k), f.p);
+}
 
 inline uint32_t shoup(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
 

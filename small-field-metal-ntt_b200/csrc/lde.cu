@@ -47,12 +47,12 @@ struct ExpandArgs {
   uint32_t log_q;      // added bits
 };
 
-template <Kind KD, int P, int LT>
+template <class F, Kind KD, int P, int LT>
 struct Expand {
   static constexpr int CB = P + LT;
   static constexpr int R = CB < 4 ? CB : 4;
-  using Inv = Pass<BabyBear, false, KD, P, LT, R>;
-  using Fwd = Pass<BabyBear, true, KD, P, LT, R>;
+  using Inv = Pass<F, false, KD, P, LT, R>;
+  using Fwd = Pass<F, true, KD, P, LT, R>;
   static constexpr int K = Inv::K;
   static constexpr int E = Inv::E;
   static constexpr int NT = Inv::NT;
@@ -93,7 +93,7 @@ struct Expand {
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const uint2 w = __ldg(&mq[pos_of(g, ct | M::cm(m), ai)]);
-        v[m] = mul_shoup<BabyBear>(x[m], w.x, w.y);
+        v[m] = mul_shoup<F>(x[m], w.x, w.y);
       }
       __syncthreads();  // the previous block's last shared-memory reads are done
       Fwd::template rounds_from<0>(sm, v, g, af, tid);  // forward starts in round K-1's layout
@@ -106,26 +106,23 @@ struct Expand {
   }
 };
 
-template <Kind KD, int P, int LT>
-__global__ void __launch_bounds__(Expand<KD, P, LT>::NT) expand_kernel(ExpandArgs ea) {
-  Expand<KD, P, LT>::run(ea);
+template <class F, Kind KD, int P, int LT>
+__global__ void __launch_bounds__(Expand<F, KD, P, LT>::NT) expand_kernel(ExpandArgs ea) {
+  Expand<F, KD, P, LT>::run(ea);
 }
 
-template <Kind KD, int P, int LT>
-constexpr int CB_of() { return P + LT; }
-
-template <Kind KD, int P, int LT>
+template <class F, Kind KD, int P, int LT>
 Status launch_expand(sfntt_ctx* ctx, const ExpandArgs& ea, uint32_t tiles, cudaStream_t s) {
-  using X = Expand<KD, P, LT>;
+  using X = Expand<F, KD, P, LT>;
   constexpr int smem = X::SMEM_WORDS * 4;
-  auto kern = expand_kernel<KD, P, LT>;
+  auto kern = expand_kernel<F, KD, P, LT>;
   static std::atomic<uint64_t> smem_done{0};
   if (smem > 48 * 1024) SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   launch_begin(ctx, s);
   kern<<<tiles, X::NT, smem, s>>>(ea);
   // reads 2^CB points per tile, writes 2^(CB + added_bits)
-  const uint64_t bytes = ((uint64_t)tiles << (CB_of<KD, P, LT>() + 2)) * (1u + (1u << ea.log_q));
-  static const std::string name = std::string("bb_lde_expand_") + (KD == Kind::C ? "C" : "S") + std::to_string(P);
+  const uint64_t bytes = ((uint64_t)tiles << (X::CB + 2)) * (1u + (1u << ea.log_q));
+  static const std::string name = std::string(F::kTag) + "_lde_expand_" + (KD == Kind::C ? "C" : "S") + std::to_string(P);
   return launch_check(ctx, name.c_str(), s, bytes);
 }
 
@@ -135,11 +132,12 @@ __host__ __device__ constexpr int x_lt_s(int P) { return P <= 10 ? 3 : 13 - P; }
 #define SFNTT_X_CASE(PP)                                                                       \
   case PP:                                                                                     \
     if (contiguous) {                                                                          \
-      if (full) return launch_expand<Kind::C, PP, kCTileBits - PP>(ctx, ea, tiles_full, s);   \
-      return launch_expand<Kind::C, PP, 0>(ctx, ea, tiles_single, s);                         \
+      if (full) return launch_expand<F, Kind::C, PP, kCTileBits - PP>(ctx, ea, tiles_full, s); \
+      return launch_expand<F, Kind::C, PP, 0>(ctx, ea, tiles_single, s);                       \
     }                                                                                          \
-    return launch_expand<Kind::S, PP, x_lt_s(PP)>(ctx, ea, tiles_s, s);
+    return launch_expand<F, Kind::S, PP, x_lt_s(PP)>(ctx, ea, tiles_s, s);
 
+template <class F>
 Status run_expand(sfntt_ctx* ctx, ExpandArgs ea, int P, uint32_t batch, cudaStream_t s) {
   const bool contiguous = ea.inv.lo == 0;
   const uint32_t log_n = ea.inv.log_n;
@@ -174,7 +172,7 @@ __global__ void replicate_kernel(uint32_t* d, uint32_t log_n, uint32_t log_ext, 
   }
 }
 
-// mul: BabyBear multiplier table M_q; scale_w: M31's n^-1 (canonical).
+// mul: BabyBear / KoalaBear multiplier table M_q; scale_w: M31's n^-1 (canonical).
 template <class F, int P, bool PLAIN, bool LSTAGE = false>
 Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_stride, uint32_t* d_out, uint32_t log_n,
                          uint32_t batch, uint32_t added_bits, const uint2* tw_inv, const uint2* tw_fwd,
@@ -205,7 +203,7 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   launch_begin(ctx, s);
   SFNTT_CU(launch_pdl(kern, grid, X::NT, smem, s, pdl_fits(grid), min, mout, a));
   static const std::string name =
-      std::string(F::kMontgomery ? "bb" : "m31") + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "") +
+      std::string(F::kTag) + "_lde_expand_tma_S" + std::to_string(P) + (PLAIN ? "p" : "") +
       (LSTAGE ? "c" : "");
   return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
 }
@@ -215,19 +213,23 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
 namespace {
 
 // Input columns at stride in_stride (n, or n_ext when they already sit in the
-// output columns); output bit-reversed rows.
-Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uint32_t* d_out, uint32_t log_n,
-                   uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+// output columns); output bit-reversed rows.  F is BabyBear or KoalaBear.
+template <class F>
+Status monty_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uint32_t* d_out, uint32_t log_n,
+                      uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+  constexpr int field = F::kId;
+  const host::MontyField& mf = host::monty_field(field);
   const uint32_t log_ext = log_n + added_bits;
-  if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
+  if (log_ext + 1 > mf.two_adicity)
+    return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(mf.two_adicity - 1)};
   if (batch == 0) return {};
   const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
   const bool fused = mode == SFNTT_LDE_FUSED && log_n >= 1 && log_n <= 24 && added_bits <= 4;
   if (fused) {
     const uint2 *tw_inv = nullptr, *tw_fwd = nullptr, *mul = nullptr;
-    SFNTT_TRY(bb_twiddles(ctx, true, log_n, s, &tw_inv));
-    SFNTT_TRY(bb_twiddles(ctx, false, log_ext, s, &tw_fwd));
-    SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 0, s, &mul));
+    SFNTT_TRY(monty_twiddles(ctx, field, true, log_n, s, &tw_inv));
+    SFNTT_TRY(monty_twiddles(ctx, field, false, log_ext, s, &tw_fwd));
+    SFNTT_TRY(monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 0, s, &mul));
     const bool tma_ok = !ctx->no_tma && log_n >= 13 && aligned16(d_in) && aligned16(d_out);
     if (tma_ok) {
       // I1: inverse layers [0, lo) into the output buffer, ending with the
@@ -239,23 +241,23 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
       const uint2 *tw_i = nullptr, *tw_f = nullptr;
       const bool plain = ctx->lde_plain;
       if (plain) {
-        SFNTT_TRY(bb_twist_table(ctx, lo, 8, true, s, &tw_i));
-        SFNTT_TRY(bb_twist_table(ctx, lo, 8, false, s, &tw_f));
+        SFNTT_TRY(monty_twist_table(ctx, field, lo, 8, true, s, &tw_i));
+        SFNTT_TRY(monty_twist_table(ctx, field, lo, 8, false, s, &tw_f));
       }
       const uint32_t mask = (uint32_t)(n - 1);
-      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, true, d_in, d_out, in_stride, n_ext, log_n, batch, 0, lo, 0u, tw_inv,
-                           s, tw_i, mask));
+      SFNTT_TRY(layers_dev(ctx, field, true, d_in, d_out, in_stride, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s, tw_i,
+                           mask));
       if (plain)
-        SFNTT_TRY((launch_tma_expand<BabyBear, 8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
-                                                        tw_fwd, mul, s)));
+        SFNTT_TRY((launch_tma_expand<F, 8, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd,
+                                                 mul, s)));
       else if (batch >= 16)  // the chunk's twiddles are reused across >= 16 columns
-        SFNTT_TRY((launch_tma_expand<BabyBear, 8, false, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits,
-                                                               tw_inv, tw_fwd, mul, s)));
+        SFNTT_TRY((launch_tma_expand<F, 8, false, true>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
+                                                        tw_fwd, mul, s)));
       else
-        SFNTT_TRY((launch_tma_expand<BabyBear, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv,
-                                                         tw_fwd, mul, s)));
-      SFNTT_TRY(layers_dev(ctx, SFNTT_BABYBEAR, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd,
-                           s, tw_f, mask));
+        SFNTT_TRY((launch_tma_expand<F, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd,
+                                                  mul, s)));
+      SFNTT_TRY(layers_dev(ctx, field, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd, s, tw_f,
+                           mask));
       return {};
     }
     const uint32_t lo = log_n <= 12 ? 0u : (log_n + 1) / 2;
@@ -265,7 +267,7 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
       r.args.in = d_in; r.args.out = d_out; r.args.tw = tw_inv;
       r.args.in_stride = in_stride; r.args.out_stride = n_ext;
       r.args.log_n = log_n; r.args.lo = 0; r.P = (int)lo; r.contiguous = true; r.batch = batch;
-      SFNTT_TRY(run_pass_bb_inv(ctx, r, s));
+      SFNTT_TRY(run_pass_field(ctx, field, false, r, s));
     }
     ExpandArgs ea{};
     ea.inv.in = lo > 0 ? d_out : d_in;
@@ -278,13 +280,13 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
     ea.tw_fwd = tw_fwd;
     ea.mul = mul;
     ea.log_q = added_bits;
-    SFNTT_TRY(run_expand(ctx, ea, P, batch, s));
+    SFNTT_TRY(run_expand<F>(ctx, ea, P, batch, s));
     if (lo > 0) {  // F3: forward layers [0, lo) of the n_ext network
       PassRequest r{};
       r.args.in = d_out; r.args.out = d_out; r.args.tw = tw_fwd;
       r.args.in_stride = n_ext; r.args.out_stride = n_ext;
       r.args.log_n = log_ext; r.args.lo = 0; r.P = (int)lo; r.contiguous = true; r.batch = batch;
-      SFNTT_TRY(run_pass_bb_fwd(ctx, r, s));
+      SFNTT_TRY(run_pass_field(ctx, field, true, r, s));
     }
     return {};
   }
@@ -294,16 +296,16 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
   SFNTT_TRY(ctx->buf_aux.reserve(bytes));
   uint32_t* coeffs = ctx->buf_aux.as<uint32_t>();
   if (log_n > 0) {
-    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_BABYBEAR, true, d_in, coeffs, in_stride, n, log_n, batch, false, s));
-    SFNTT_TRY(scale_dev(ctx, SFNTT_BABYBEAR, coeffs, n * batch, host::invmod((uint32_t)n, host::BB_P), s));
+    SFNTT_TRY(ntt_dev_oop(ctx, field, true, d_in, coeffs, in_stride, n, log_n, batch, false, s));
+    SFNTT_TRY(scale_dev(ctx, field, coeffs, n * batch, host::invmod((uint32_t)n, mf.p), s));
   } else {
     SFNTT_CU(cudaMemcpy2DAsync(coeffs, 4, d_in, in_stride * 4, 4, batch, cudaMemcpyDeviceToDevice, s));
   }
   SFNTT_TRY(zero_pad_dev(ctx, coeffs, d_out, log_n, batch, added_bits, s));
   const uint2* shift_tab = nullptr;
-  SFNTT_TRY(bb_lde_table(ctx, log_n, added_bits, shift_monty, 1, s, &shift_tab));
-  SFNTT_TRY(mul_table_dev(ctx, d_out, log_ext, batch, shift_tab, s));
-  if (log_ext > 0) SFNTT_TRY(ntt_dev(ctx, SFNTT_BABYBEAR, SFNTT_V4_CT_GS_R4, false, d_out, log_ext, batch, s));
+  SFNTT_TRY(monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 1, s, &shift_tab));
+  SFNTT_TRY(mul_table_dev(ctx, field, d_out, log_ext, batch, shift_tab, s));
+  if (log_ext > 0) SFNTT_TRY(ntt_dev(ctx, field, SFNTT_V4_CT_GS_R4, false, d_out, log_ext, batch, s));
   return {};
 }
 
@@ -314,19 +316,25 @@ Status bb_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, uin
 // natural-order input and output; the input columns are bit-reversed into the
 // output columns, the LDE runs there in place, and the output columns are
 // bit-reversed in place.
-Status bb_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
-                  uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n,
+                     uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
+  if (!is_monty(field)) return {SFNTT_INVALID_ARGUMENT, "coset LDE needs BabyBear or KoalaBear"};
   if (mode & ~(SFNTT_LDE_UNFUSED | SFNTT_LDE_NATURAL)) return {SFNTT_INVALID_ARGUMENT, "unknown LDE mode"};
   const int form = mode & SFNTT_LDE_UNFUSED;
-  if (!(mode & SFNTT_LDE_NATURAL))
-    return bb_lde_rows(ctx, d_in, 1ull << log_n, d_out, log_n, batch, added_bits, shift_monty, form, s);
-  const uint32_t log_ext = log_n + added_bits;
-  if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
-  if (batch == 0) return {};
-  const uint64_t n_ext = 1ull << log_ext;
-  SFNTT_TRY(bitrev_cols_dev(ctx, d_in, 1ull << log_n, d_out, n_ext, log_n, batch, s));
-  SFNTT_TRY(bb_lde_rows(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, shift_monty, form, s));
-  return bitrev_cols_dev(ctx, d_out, n_ext, d_out, n_ext, log_ext, batch, s);
+  return with_monty(field, [&](auto fld) -> Status {
+    using F = decltype(fld);
+    if (!(mode & SFNTT_LDE_NATURAL))
+      return monty_lde_rows<F>(ctx, d_in, 1ull << log_n, d_out, log_n, batch, added_bits, shift_monty, form, s);
+    const host::MontyField& mf = host::monty_field(field);
+    const uint32_t log_ext = log_n + added_bits;
+    if (log_ext + 1 > mf.two_adicity)
+      return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(mf.two_adicity - 1)};
+    if (batch == 0) return {};
+    const uint64_t n_ext = 1ull << log_ext;
+    SFNTT_TRY(bitrev_cols_dev(ctx, d_in, 1ull << log_n, d_out, n_ext, log_n, batch, s));
+    SFNTT_TRY(monty_lde_rows<F>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, shift_monty, form, s));
+    return bitrev_cols_dev(ctx, d_out, n_ext, d_out, n_ext, log_ext, batch, s);
+  });
 }
 
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,

@@ -66,9 +66,10 @@ Status scratch_address(int device, uint32_t** out) {
 // Cached twiddles only: never generates (generation allocates).
 Status resident_twiddles(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, const uint2** tw) {
   const int d = inverse ? 1 : 0;
-  if (field == SFNTT_BABYBEAR) {
-    if (ctx->bb_tw[d].p && ctx->bb_log[d] >= log_n) {
-      *tw = ctx->bb_tw[d].as<uint2>();
+  if (is_monty(field)) {
+    const int k = monty_slot(field);
+    if (ctx->monty_tw[k][d].p && ctx->monty_log[k][d] >= log_n) {
+      *tw = ctx->monty_tw[k][d].as<uint2>();
       return {};
     }
   } else {
@@ -93,8 +94,8 @@ extern "C" int sfntt_stockham_noalloc(sfntt_ctx* ctx, int field, int inverse, ui
   if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
   if (prev != ctx->device) cudaSetDevice(ctx->device);
   auto run = [&]() -> Status {
-    if (field != SFNTT_BABYBEAR && field != SFNTT_M31) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
-    if ((field == SFNTT_BABYBEAR && log_n > host::BB_TWO_ADICITY) || (field == SFNTT_M31 && log_n > 30))
+    if (!valid_field(field)) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
+    if ((is_monty(field) && log_n > host::monty_field(field).two_adicity) || (field == SFNTT_M31 && log_n > 30))
       return {SFNTT_INVALID_SIZE, "log_n exceeds the field's maximum"};
     const uint64_t words = (uint64_t)batch << log_n;
     if (words > kNoAllocMaxWords)

@@ -14,6 +14,7 @@ namespace sfntt {
 
 static Status run_tma_pass(sfntt_ctx* ctx, int field, bool desc, const TmaRequest& r, cudaStream_t s) {
   if (field == SFNTT_BABYBEAR) return desc ? run_tma_pass_bb_fwd(ctx, r, s) : run_tma_pass_bb_inv(ctx, r, s);
+  if (field == SFNTT_KOALABEAR) return desc ? run_tma_pass_kb_fwd(ctx, r, s) : run_tma_pass_kb_inv(ctx, r, s);
   return desc ? run_tma_pass_m31_fwd(ctx, r, s) : run_tma_pass_m31_inv(ctx, r, s);
 }
 
@@ -30,11 +31,6 @@ static int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
   return (int)(1 + s);
 }
 
-static Status run_pass(sfntt_ctx* ctx, int field, bool desc, const PassRequest& r, cudaStream_t s) {
-  if (field == SFNTT_BABYBEAR) return desc ? run_pass_bb_fwd(ctx, r, s) : run_pass_bb_inv(ctx, r, s);
-  return desc ? run_pass_m31_fwd(ctx, r, s) : run_pass_m31_inv(ctx, r, s);
-}
-
 // Split layers [a, b) into passes of at most 12 layers, as even as possible,
 // the lowest pass taking the remainder.  Returns the number of passes.
 static int split_layers(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
@@ -47,12 +43,12 @@ static int split_layers(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4])
 }
 
 static Status get_tw(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, cudaStream_t s, const uint2** tw) {
-  if (field == SFNTT_BABYBEAR) return bb_twiddles(ctx, inverse, log_n, s, tw);
+  if (is_monty(field)) return monty_twiddles(ctx, field, inverse, log_n, s, tw);
   return m31_twiddles(ctx, inverse, log_n, s, tw);
 }
 
 static uint32_t inv_n_canonical(int field, uint32_t log_n) {
-  const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
+  const uint32_t p = host::field_p(field);
   return host::invmod(host::powmod(2, log_n, p), p);
 }
 
@@ -84,7 +80,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
       r.scale_w = (i == kt - 1) ? scale_w : 0u;
       ok = tma_pass_ok(r);
     }
-    if (ok && field == SFNTT_BABYBEAR) {
+    if (ok && is_monty(field)) {
       // Strided passes either use per-position twiddles (self-contained) or,
       // when `plain`, run plain sub-transforms whose four-step twist is applied
       // by a neighbour: forward -> the next pass at its load, inverse -> the
@@ -101,7 +97,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
         }
         if (!plain) continue;
         const int nb = pi + 1;  // the strided chunk just above pi
-        SFNTT_TRY(bb_twist_table(ctx, lo[nb], cnt[nb], inverse, s, &req[i].twist));
+        SFNTT_TRY(monty_twist_table(ctx, field, lo[nb], cnt[nb], inverse, s, &req[i].twist));
         req[i].twist_mask = (1u << (lo[nb] + cnt[nb])) - 1u;
       }
     }
@@ -112,7 +108,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
   }
   if (edge_twist) return {SFNTT_INVALID_ARGUMENT, "a boundary twist needs the TMA engine"};
   const int k = split_layers(a, b, lo, cnt);
-  const uint32_t p = field == SFNTT_BABYBEAR ? host::BB_P : host::M31_P;
+  const uint32_t p = host::field_p(field);
   for (int i = 0; i < k; ++i) {
     const int pi = inverse ? i : (k - 1 - i);  // forward runs the high layers first
     PassRequest r{};
@@ -129,7 +125,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
     r.P = (int)cnt[pi];
     r.contiguous = (lo[pi] == 0);
     r.batch = batch;
-    SFNTT_TRY(run_pass(ctx, field, !inverse, r, s));
+    SFNTT_TRY(run_pass_field(ctx, field, !inverse, r, s));
   }
   return {};
 }
@@ -180,24 +176,26 @@ static Status launch_layer(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, co
   launch_begin(ctx, s);
   layer_kernel<F, DESC><<<blocks, 256, 0, s>>>(in, out, tw, log_n, L, pairs, scale_w ? 1u : 0u, scale_w,
                                                  host::shoup(scale_w, F::P));
-  return launch_check(ctx, F::kMontgomery ? "bb_layer" : "m31_layer", s, pairs * 16u);
+  static const std::string name = std::string(F::kTag) + "_layer";
+  return launch_check(ctx, name.c_str(), s, pairs * 16u);
 }
 
 static Status layer(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, const uint2* tw,
                     uint32_t log_n, uint32_t L, uint32_t batch, uint32_t scale_w, cudaStream_t s) {
-  if (field == SFNTT_BABYBEAR)
-    return inverse ? launch_layer<BabyBear, false>(ctx, in, out, tw, log_n, L, batch, scale_w, s)
-                   : launch_layer<BabyBear, true>(ctx, in, out, tw, log_n, L, batch, scale_w, s);
-  return inverse ? launch_layer<M31, false>(ctx, in, out, tw, log_n, L, batch, scale_w, s)
-                 : launch_layer<M31, true>(ctx, in, out, tw, log_n, L, batch, scale_w, s);
+  return with_field(field, [&](auto fld) {
+    using F = decltype(fld);
+    return inverse ? launch_layer<F, false>(ctx, in, out, tw, log_n, L, batch, scale_w, s)
+                   : launch_layer<F, true>(ctx, in, out, tw, log_n, L, batch, scale_w, s);
+  });
 }
 
 // ----------------------------------------------------------------- driver ---
 Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d, uint32_t log_n, uint32_t batch,
                cudaStream_t s) {
-  if (field != SFNTT_BABYBEAR && field != SFNTT_M31) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
+  if (!valid_field(field)) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
   if (variant < SFNTT_BEST || variant > SFNTT_V4_CT_GS_R4) return {SFNTT_INVALID_ARGUMENT, "unknown variant"};
-  if (field == SFNTT_BABYBEAR && log_n > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n > 27"};
+  if (is_monty(field) && log_n > host::monty_field(field).two_adicity)
+    return {SFNTT_INVALID_SIZE, "log_n > " + std::to_string(host::monty_field(field).two_adicity)};
   if (field == SFNTT_M31 && log_n > 30) return {SFNTT_INVALID_SIZE, "log_n > 30"};
   if (log_n >= 32 || ((uint64_t)batch << log_n) >= (1ull << 40)) return {SFNTT_INVALID_SIZE, "too large"};
   if (variant == SFNTT_V1_CT_DIT_R2 && inverse)
@@ -292,9 +290,10 @@ __global__ void pointwise_kernel(const uint32_t* a, const uint32_t* b, uint32_t*
     out[i] = mul_var<F>(a[i], b[i]);
 }
 
+template <class F>
 __global__ void monty_kernel(uint32_t* d, uint64_t n, int to) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    d[i] = to ? mul_var<BabyBear>(d[i], BabyBear::R2) : mul_var<BabyBear>(d[i], 1u);
+    d[i] = to ? mul_var<F>(d[i], F::R2) : mul_var<F>(d[i], 1u);
 }
 
 // out[c * n_ext + r] = r < n ? in[c * n + r] : 0   (bb_zero_pad_batch, shaders/babybear/bb_ntt_r2.metal:379-398)
@@ -308,10 +307,11 @@ __global__ void zero_pad_kernel(const uint32_t* __restrict__ in, uint32_t* __res
 }
 
 // d[c * n_ext + i] *= tab[i]   (bb_coset_shift_batch, shaders/babybear/bb_ntt_r2.metal:402-415)
+template <class F>
 __global__ void mul_table_kernel(uint32_t* d, uint32_t log_ext, uint64_t total, const uint2* __restrict__ tab) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint2 w = tab[i & ((1ull << log_ext) - 1ull)];
-    d[i] = mul_shoup<BabyBear>(d[i], w.x, w.y);
+    d[i] = mul_shoup<F>(d[i], w.x, w.y);
   }
 }
 
@@ -325,10 +325,11 @@ uint32_t grid_for(sfntt_ctx* ctx, uint64_t n) {
 
 Status scale_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint64_t n, uint32_t w, cudaStream_t s) {
   launch_begin(ctx, s);
-  if (field == SFNTT_BABYBEAR)
-    scale_kernel<BabyBear><<<grid_for(ctx, n), 256, 0, s>>>(d, n, w, host::shoup(w, host::BB_P));
-  else
-    scale_kernel<M31><<<grid_for(ctx, n), 256, 0, s>>>(d, n, w, host::shoup(w, host::M31_P));
+  with_field(field, [&](auto fld) {
+    using F = decltype(fld);
+    scale_kernel<F><<<grid_for(ctx, n), 256, 0, s>>>(d, n, w, host::shoup(w, F::P));
+    return 0;
+  });
   return launch_check(ctx, "scale", s, n * 8u);
 }
 
@@ -336,16 +337,22 @@ Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uin
                          cudaStream_t s) {
   if (n == 0) return {};
   launch_begin(ctx, s);
-  if (field == SFNTT_BABYBEAR) pointwise_kernel<BabyBear><<<grid_for(ctx, n), 256, 0, s>>>(a, b, out, n);
-  else pointwise_kernel<M31><<<grid_for(ctx, n), 256, 0, s>>>(a, b, out, n);
+  with_field(field, [&](auto fld) {
+    pointwise_kernel<decltype(fld)><<<grid_for(ctx, n), 256, 0, s>>>(a, b, out, n);
+    return 0;
+  });
   return launch_check(ctx, "pointwise_mul", s, (uint64_t)n * 12u);
 }
 
-Status bb_monty_dev(sfntt_ctx* ctx, bool to, uint32_t* d, size_t n, cudaStream_t s) {
+Status monty_convert_dev(sfntt_ctx* ctx, int field, bool to, uint32_t* d, size_t n, cudaStream_t s) {
+  if (!is_monty(field)) return {SFNTT_INVALID_ARGUMENT, "Montgomery conversion needs BabyBear or KoalaBear"};
   if (n == 0) return {};
   launch_begin(ctx, s);
-  monty_kernel<<<grid_for(ctx, n), 256, 0, s>>>(d, n, to ? 1 : 0);
-  return launch_check(ctx, to ? "bb_to_monty" : "bb_from_monty", s, (uint64_t)n * 8u);
+  with_monty(field, [&](auto fld) {
+    monty_kernel<decltype(fld)><<<grid_for(ctx, n), 256, 0, s>>>(d, n, to ? 1 : 0);
+    return 0;
+  });
+  return launch_check(ctx, to ? "to_monty" : "from_monty", s, (uint64_t)n * 8u);
 }
 
 Status zero_pad_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t log_n, uint32_t batch,
@@ -356,12 +363,15 @@ Status zero_pad_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t 
   return launch_check(ctx, "bb_zero_pad", s, total * 4u + ((uint64_t)batch << log_n) * 4u);
 }
 
-Status mul_table_dev(sfntt_ctx* ctx, uint32_t* d, uint32_t log_ext, uint32_t batch, const uint2* tab,
+Status mul_table_dev(sfntt_ctx* ctx, int field, uint32_t* d, uint32_t log_ext, uint32_t batch, const uint2* tab,
                      cudaStream_t s) {
   const uint64_t total = (uint64_t)batch << log_ext;
   launch_begin(ctx, s);
-  mul_table_kernel<<<grid_for(ctx, total), 256, 0, s>>>(d, log_ext, total, tab);
-  return launch_check(ctx, "bb_coset_shift", s, total * 8u);
+  with_monty(field, [&](auto fld) {
+    mul_table_kernel<decltype(fld)><<<grid_for(ctx, total), 256, 0, s>>>(d, log_ext, total, tab);
+    return 0;
+  });
+  return launch_check(ctx, "coset_shift", s, total * 8u);
 }
 
 }  // namespace sfntt

@@ -25,7 +25,7 @@ struct PassRequest {
 // Kernel label for timing / profiles, e.g. "bb_fwd_pass_S10".
 template <class F, bool DESC, Kind KD, int P>
 const char* pass_name() {
-  static const std::string n = std::string(F::kMontgomery ? "bb_" : "m31_") + (DESC ? "fwd" : "inv") +
+  static const std::string n = std::string(F::kTag) + "_" + (DESC ? "fwd" : "inv") +
                                "_pass_" + (KD == Kind::C ? "C" : "S") + std::to_string(P);
   return n.c_str();
 }
@@ -90,7 +90,15 @@ Status run_pass_impl(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s) {
 // One entry per (field, direction); defined in ntt_pass_*.cu.
 Status run_pass_bb_fwd(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
 Status run_pass_bb_inv(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
+Status run_pass_kb_fwd(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
+Status run_pass_kb_inv(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
 Status run_pass_m31_fwd(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
 Status run_pass_m31_inv(sfntt_ctx* ctx, const PassRequest& req, cudaStream_t s);
+
+inline Status run_pass_field(sfntt_ctx* ctx, int field, bool desc, const PassRequest& r, cudaStream_t s) {
+  if (field == SFNTT_BABYBEAR) return desc ? run_pass_bb_fwd(ctx, r, s) : run_pass_bb_inv(ctx, r, s);
+  if (field == SFNTT_KOALABEAR) return desc ? run_pass_kb_fwd(ctx, r, s) : run_pass_kb_inv(ctx, r, s);
+  return desc ? run_pass_m31_fwd(ctx, r, s) : run_pass_m31_inv(ctx, r, s);
+}
 
 }  // namespace sfntt

@@ -1,0 +1,8 @@
+// Instantiates the persistent TMA passes for KoalaBear, inv direction.
+#include "tma_launch.cuh"
+
+namespace sfntt {
+Status run_tma_pass_kb_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
+  return run_tma_pass_impl<KoalaBear, false>(ctx, r, s);
+}
+}  // namespace sfntt

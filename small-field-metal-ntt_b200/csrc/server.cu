@@ -112,10 +112,11 @@ size_t out_bytes(const sfntt_lde_item& it) { return ((size_t)it.batch << (it.log
 size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
 size_t arena_bytes(const Request& r) { return (r.h_in ? round256(in_bytes(r.item)) : 0) + out_bytes(r.item); }
 
-// BabyBear items outside the fused LDE's range run the unfused composition
-// through the context's one scratch buffer, so they run alone on the device.
+// BabyBear / KoalaBear items outside the fused LDE's range run the unfused
+// composition through the context's one scratch buffer, so they run alone on
+// the device.
 bool exclusive(const sfntt_lde_item& it) {
-  return it.field == SFNTT_BABYBEAR && it.batch && !(it.log_n >= 1 && it.log_n <= 24 && it.added_bits <= 4);
+  return sfntt::is_monty(it.field) && it.batch && !(it.log_n >= 1 && it.log_n <= 24 && it.added_bits <= 4);
 }
 
 Status admit(sfntt_server* sv) {
@@ -256,7 +257,7 @@ namespace {
 int submit(sfntt_server* sv, const sfntt_lde_item* req, const uint32_t* h_in, uint32_t* h_out, uint64_t* ticket) {
   if (!sv || !req || !ticket) return SFNTT_INVALID_ARGUMENT;
   std::lock_guard<std::recursive_mutex> lk(sv->ctx->mu);
-  if (req->field != SFNTT_BABYBEAR && req->field != SFNTT_M31) return SFNTT_INVALID_ARGUMENT;
+  if (!sfntt::valid_field(req->field)) return SFNTT_INVALID_ARGUMENT;
   Request r;
   r.item = *req;
   r.h_in = h_in;

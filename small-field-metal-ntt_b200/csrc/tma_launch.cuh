@@ -73,7 +73,7 @@ inline Status encode_s_map(CUtensorMap* m, const uint32_t* base, uint32_t lo, in
 
 template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
 const char* tma_pass_name() {
-  static const std::string nm = std::string(F::kMontgomery ? "bb_" : "m31_") + (DESC ? "fwd" : "inv") +
+  static const std::string nm = std::string(F::kTag) + "_" + (DESC ? "fwd" : "inv") +
                                 "_tma_" + (KD == Kind::C ? "C" : "S") + std::to_string(P) + (PLAIN ? "p" : "") +
                                 (TW ? "t" : "");
   return nm.c_str();
@@ -117,7 +117,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
 }
 
-// BabyBear instantiates the twist / plain variants; M31 never needs them.
+// BabyBear and KoalaBear instantiate the twist / plain variants; M31 never needs them.
 #define SFNTT_TMA_C(PP)                                                                          \
   case PP:                                                                                       \
     if constexpr (F::kMontgomery) {                                                              \
@@ -157,6 +157,8 @@ Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
 
 Status run_tma_pass_bb_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 Status run_tma_pass_bb_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+Status run_tma_pass_kb_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
+Status run_tma_pass_kb_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 Status run_tma_pass_m31_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 Status run_tma_pass_m31_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 

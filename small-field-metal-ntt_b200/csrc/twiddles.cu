@@ -4,13 +4,15 @@
 // BabyBear layer s holds g_{s+1}^j, j < 2^s, with g_k = two_adic_generator(k)
 // (src/field/babybear.rs:83-97); the inverse table holds g_{s+1}^-j
 // (src/ntt/babybear/twiddles.rs:13-19).  The tables for all s are nested, so
-// one table up to the largest log n serves every smaller size.
+// one table up to the largest log n serves every smaller size.  KoalaBear
+// tables are built the same way from its own two_adic_generator.
 //
 // M31 layer l holds the x coordinate (y on the last layer) of the l-times
 // doubled Coset::odds(log n) at bit-reversed positions; the inverse table holds
 // their field inverses (src/ntt/m31/twiddles.rs:19-68).
 //
 // Entries are stored as Shoup pairs (w, floor(w 2^32 / p)) with w canonical.
+#include <string>
 #include <vector>
 
 #include "context.hpp"
@@ -20,15 +22,16 @@
 namespace sfntt {
 namespace {
 
-struct BbGens { uint32_t g[28]; };  // Montgomery-form generator per layer (index s: g_{s+1}^(+-1))
+struct MontyGens { uint32_t g[28]; };  // Montgomery-form generator per layer (index s: g_{s+1}^(+-1))
 
-__global__ void bb_twiddle_kernel(uint2* tab, uint32_t count, BbGens gens) {
+template <class F>
+__global__ void monty_twiddle_kernel(uint2* tab, uint32_t count, MontyGens gens) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const uint32_t s = 31u - __clz(t + 1u);
   const uint32_t j = t + 1u - (1u << s);
-  const uint32_t w = to_canonical(BabyBear{}, pow_var<BabyBear>(gens.g[s], j));
-  tab[t] = make_uint2(w, shoup_of<BabyBear>(w));
+  const uint32_t w = to_canonical(F{}, pow_var<F>(gens.g[s], j));
+  tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
 struct M31Layers {
@@ -72,16 +75,17 @@ __global__ void m31_twiddle_kernel(uint2* tab, uint32_t log_n, M31Layers L, int 
 struct LdeBases { uint32_t b[16]; };
 
 // kind 0: tab[q*n + i] = n^-1 * base_q^i ; kind 1: tab[i] = base_0^i
-__global__ void bb_power_table_kernel(uint2* tab, uint32_t log_len, uint32_t count, LdeBases bases,
-                                      uint32_t scale_monty) {
+template <class F>
+__global__ void power_table_kernel(uint2* tab, uint32_t log_len, uint32_t count, LdeBases bases,
+                                   uint32_t scale_monty) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const uint32_t q = t >> log_len;
   const uint32_t i = t & ((1u << log_len) - 1u);
-  uint32_t w = pow_var<BabyBear>(bases.b[q], i);
-  w = mul_var<BabyBear>(w, scale_monty);
-  w = to_canonical(BabyBear{}, w);
-  tab[t] = make_uint2(w, shoup_of<BabyBear>(w));
+  uint32_t w = pow_var<F>(bases.b[q], i);
+  w = mul_var<F>(w, scale_monty);
+  w = to_canonical(F{}, w);
+  tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
 // Four-step twist of a strided pass over layers [lo, lo + P) (span N =
@@ -89,15 +93,16 @@ __global__ void bb_power_table_kernel(uint2* tab, uint32_t log_len, uint32_t cou
 // reference's per-position DIF layers equal the plain 2^P-point sub-DIF
 // followed by this factor, and its DIT layers equal the plain sub-DIT applied
 // to inputs multiplied by the inverse factor.
-__global__ void bb_twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_monty) {
+template <class F>
+__global__ void twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_monty) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (1u << (lo + P))) return;
   const uint32_t l = t & ((1u << lo) - 1u);
   const uint32_t e = t >> lo;
   const uint32_t re = __brev(e) >> (32u - P);
-  uint32_t w = pow_var<BabyBear>(g_monty, l * re);
-  w = to_canonical(BabyBear{}, w);
-  tab[t] = make_uint2(w, shoup_of<BabyBear>(w));
+  uint32_t w = pow_var<F>(g_monty, l * re);
+  w = to_canonical(F{}, w);
+  tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
 Status sync_after_build(sfntt_ctx* ctx, cudaStream_t stream, const char* what) {
@@ -108,25 +113,33 @@ Status sync_after_build(sfntt_ctx* ctx, cudaStream_t stream, const char* what) {
 
 }  // namespace
 
-Status bb_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out) {
-  const int d = inverse ? 1 : 0;
-  if (log_n > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "BabyBear log_n exceeds two-adicity 27"};
-  if (ctx->bb_log[d] < log_n || ctx->bb_tw[d].p == nullptr) {
+Status monty_twiddles(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, cudaStream_t stream,
+                      const uint2** out) {
+  const host::MontyField& f = host::monty_field(field);
+  const int d = inverse ? 1 : 0, k = monty_slot(field);
+  if (log_n > f.two_adicity)
+    return {SFNTT_INVALID_SIZE, std::string(f.name) + " log_n exceeds two-adicity " + std::to_string(f.two_adicity)};
+  DevBuf& buf = ctx->monty_tw[k][d];
+  if (ctx->monty_log[k][d] < log_n || buf.p == nullptr) {
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twiddle table not prepared before capture"};
     const uint32_t want = log_n < 12 ? 12 : log_n;  // small sizes share one 4 Ki table
     const uint32_t count = (1u << want) - 1u;
-    SFNTT_TRY(ctx->bb_tw[d].reserve((size_t)count * sizeof(uint2)));
-    BbGens g{};
-    for (uint32_t s = 0; s < 27; ++s) {
-      uint32_t gen = host::bb_two_adic_generator(s + 1);
-      if (inverse) gen = host::invmod(gen, host::BB_P);
-      g.g[s] = host::bb_to_monty(gen);
+    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    MontyGens g{};
+    for (uint32_t s = 0; s < f.two_adicity; ++s) {
+      uint32_t gen = host::two_adic_generator(f, s + 1);
+      if (inverse) gen = host::invmod(gen, f.p);
+      g.g[s] = host::to_monty(f, gen);
     }
-    bb_twiddle_kernel<<<(count + 255) / 256, 256, 0, stream>>>(ctx->bb_tw[d].as<uint2>(), count, g);
-    SFNTT_TRY(sync_after_build(ctx, stream, "bb_twiddle_kernel"));
-    ctx->bb_log[d] = want;
+    with_monty(field, [&](auto fld) {
+      using F = decltype(fld);
+      monty_twiddle_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), count, g);
+      return 0;
+    });
+    SFNTT_TRY(sync_after_build(ctx, stream, "monty_twiddle_kernel"));
+    ctx->monty_log[k][d] = want;
   }
-  *out = ctx->bb_tw[d].as<uint2>();
+  *out = buf.as<uint2>();
   return {};
 }
 
@@ -155,40 +168,46 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
   return {};
 }
 
-Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty, int kind,
-                    cudaStream_t stream, const uint2** out) {
+Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
+                       int kind, cudaStream_t stream, const uint2** out) {
+  const host::MontyField& f = host::monty_field(field);
   const uint32_t log_ext = log_n + added_bits;
-  if (log_ext + 1 > host::BB_TWO_ADICITY) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 26"};
+  if (log_ext + 1 > f.two_adicity)
+    return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(f.two_adicity - 1)};
   if (kind == 0 && added_bits > 4) return {SFNTT_INVALID_ARGUMENT, "fused LDE supports added_bits <= 4"};
-  const auto key = std::make_tuple(log_n, added_bits, shift_monty, kind);
+  const auto key = std::make_tuple(monty_slot(field), log_n, added_bits, shift_monty, kind);
   auto it = ctx->lde_tabs.find(key);
   if (it == ctx->lde_tabs.end()) {
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "LDE table not prepared before capture"};
-    const uint32_t shift = shift_monty ? host::bb_from_monty(shift_monty) : host::bb_two_adic_generator(log_ext + 1);
+    const uint32_t shift = shift_monty ? host::from_monty(f, shift_monty) : host::two_adic_generator(f, log_ext + 1);
     LdeBases B{};
     uint32_t log_len, count, scale;
     if (kind == 0) {
       // quarter q of the zero-padded DIF gets g_ext^{i * rev(q)} from its top
       // added_bits layers; fold it with the shift and n^-1 into one multiplier
-      const uint32_t g_ext = host::bb_two_adic_generator(log_ext);
+      const uint32_t g_ext = host::two_adic_generator(f, log_ext);
       for (uint32_t q = 0; q < (1u << added_bits); ++q) {
         uint32_t rq = 0;
         for (uint32_t bit = 0; bit < added_bits; ++bit) rq |= ((q >> bit) & 1u) << (added_bits - 1 - bit);
-        B.b[q] = host::bb_to_monty(host::mulmod(shift, host::powmod(g_ext, rq, host::BB_P), host::BB_P));
+        B.b[q] = host::to_monty(f, host::mulmod(shift, host::powmod(g_ext, rq, f.p), f.p));
       }
       log_len = log_n;
       count = 1u << log_ext;
-      scale = host::bb_to_monty(host::invmod(1u << log_n, host::BB_P));
+      scale = host::to_monty(f, host::invmod(1u << log_n, f.p));
     } else {
-      B.b[0] = host::bb_to_monty(shift);
+      B.b[0] = host::to_monty(f, shift);
       log_len = log_ext;
       count = 1u << log_ext;
-      scale = host::bb_to_monty(1);
+      scale = host::to_monty(f, 1);
     }
     DevBuf buf;
     SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
-    bb_power_table_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_len, count, B, scale);
-    Status s = sync_after_build(ctx, stream, "bb_power_table_kernel");
+    with_monty(field, [&](auto fld) {
+      using F = decltype(fld);
+      power_table_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_len, count, B, scale);
+      return 0;
+    });
+    Status s = sync_after_build(ctx, stream, "power_table_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->lde_tabs.emplace(key, buf).first;
   }
@@ -200,19 +219,25 @@ Status bb_lde_table(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits, uint32_
 
 namespace sfntt {
 
-Status bb_twist_table(sfntt_ctx* ctx, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream, const uint2** out) {
-  if (lo + P > host::BB_TWO_ADICITY || P == 0 || P > 8) return {SFNTT_INVALID_ARGUMENT, "twist span"};
-  const auto key = std::make_tuple(lo, P, inverse ? 1u : 0u, 2);
+Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream,
+                         const uint2** out) {
+  const host::MontyField& f = host::monty_field(field);
+  if (lo + P > f.two_adicity || P == 0 || P > 8) return {SFNTT_INVALID_ARGUMENT, "twist span"};
+  const auto key = std::make_tuple(monty_slot(field), lo, P, inverse ? 1u : 0u, 2);
   auto it = ctx->lde_tabs.find(key);
   if (it == ctx->lde_tabs.end()) {
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twist table not prepared before capture"};
-    uint32_t g = host::bb_two_adic_generator(lo + P);
-    if (inverse) g = host::invmod(g, host::BB_P);
+    uint32_t g = host::two_adic_generator(f, lo + P);
+    if (inverse) g = host::invmod(g, f.p);
     const uint32_t count = 1u << (lo + P);
     DevBuf buf;
     SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
-    bb_twist_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), lo, P, host::bb_to_monty(g));
-    Status s = sync_after_build(ctx, stream, "bb_twist_kernel");
+    with_monty(field, [&](auto fld) {
+      using F = decltype(fld);
+      twist_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), lo, P, host::to_monty(f, g));
+      return 0;
+    });
+    Status s = sync_after_build(ctx, stream, "twist_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->lde_tabs.emplace(key, buf).first;
   }

@@ -26,8 +26,10 @@ from . import _ffi
 
 M31_P = 2147483647
 BB_P = 2013265921
+KB_P = 2130706433  # KoalaBear, 2^31 - 2^24 + 1
 FIELD_M31 = 0
 FIELD_BABYBEAR = 1
+FIELD_KOALABEAR = 2  # planned in the reference (README.md:20); Montgomery u32 like BabyBear
 BEST, V1, V2, V3, V4 = 0, 1, 2, 3, 4
 LDE_FUSED, LDE_UNFUSED = 0, 1
 LDE_NATURAL = 2  # flag: natural-order input and output rows (Plonky3's coset_lde_batch)
@@ -341,6 +343,23 @@ class BbCudaCtGsR4(NttBackend):
     FIELD, VARIANT, NAME = FIELD_BABYBEAR, V4, "bb-cuda-ct-gs-r4"
 
 
+# KoalaBear (no reference implementation): the BabyBear variants over KoalaBear
+class KbCudaCtDitR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_KOALABEAR, V1, "kb-cuda-ct-dit-r2"
+
+
+class KbBatchNtt(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_KOALABEAR, V2, "kb-cuda-r2"
+
+
+class KbCudaStockhamR2(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_KOALABEAR, V3, "kb-cuda-stockham-r2"
+
+
+class KbCudaCtGsR4(NttBackend):
+    FIELD, VARIANT, NAME = FIELD_KOALABEAR, V4, "kb-cuda-ct-gs-r4"
+
+
 # reference type names (src/ntt/m31/*, src/ntt/babybear/*, src/ntt/metal_r2.rs:337-340)
 MetalCtDitR2, MetalCtGsR2, MetalStockhamR2, MetalCtGsR4 = CudaCtDitR2, CudaCtGsR2, CudaStockhamR2, CudaCtGsR4
 BbMetalCtDitR2, BbMetalR2, BbMetalStockhamR2, BbMetalCtGsR4 = BbCudaCtDitR2, BbBatchNtt, BbCudaStockhamR2, BbCudaCtGsR4
@@ -356,6 +375,8 @@ class LdeResult:
 
 class CosetLdeBatch:
     """CosetLdeBatch (src/lde/mod.rs:15-107)."""
+
+    FIELD = FIELD_BABYBEAR
 
     def __init__(self, ctx: Context | None = None, device: int = 0, fused: bool = True, natural: bool = False):
         """natural=True: natural-order input evaluations and output rows
@@ -373,19 +394,27 @@ class CosetLdeBatch:
         n_out = batch_size << (log_n + added_bits)
         dst = out if out is not None else np.empty(n_out, dtype=np.uint32)
         ns = ctypes.c_uint64()
-        st = _ffi.lib().sfntt_bb_coset_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits,
-                                           shift_monty, self.mode, _p(dst), ctypes.byref(ns))
+        st = _ffi.lib().sfntt_coset_lde(self.ctx.handle, self.FIELD, _p(inp), inp.size, log_n, batch_size,
+                                        added_bits, shift_monty, self.mode, _p(dst), ctypes.byref(ns))
         _check(self.ctx.handle, st, inp.size)
         return LdeResult(dst, int(ns.value))
 
     def execute_dev(self, in_ptr: int, out_ptr: int, log_n: int, batch_size: int, added_bits: int,
                     shift_monty: int = 0, stream: int = 0) -> None:
-        st = _ffi.lib().sfntt_bb_coset_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits,
-                                               shift_monty, self.mode, stream)
+        st = _ffi.lib().sfntt_coset_lde_dev(self.ctx.handle, self.FIELD, in_ptr, out_ptr, log_n, batch_size,
+                                            added_bits, shift_monty, self.mode, stream)
         _check(self.ctx.handle, st, batch_size << log_n)
 
     def device_info(self) -> str:
         return self.ctx.device_info()
+
+
+class KbCosetLdeBatch(CosetLdeBatch):
+    """The coset LDE over KoalaBear (no reference implementation): the
+    BabyBear algorithm with KoalaBear's constants; shift_monty 0 selects
+    two_adic_generator(log_n + added_bits + 1), log_n + added_bits <= 23."""
+
+    FIELD = FIELD_KOALABEAR
 
 
 class M31Lde:
@@ -410,6 +439,13 @@ class M31Lde:
                     stream: int = 0) -> None:
         st = _ffi.lib().sfntt_m31_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits, stream)
         _check(self.ctx.handle, st, batch_size << log_n)
+
+
+def convert_monty_dev(ctx: Context, field: int, ptr: int, n: int, to_monty: bool, stream: int = 0) -> None:
+    """In-place canonical <-> Montgomery conversion of n device words
+    (BabyBear::to_monty / from_monty, src/field/babybear.rs:54-65; KoalaBear alike)."""
+    fn = _ffi.lib().sfntt_to_monty_dev if to_monty else _ffi.lib().sfntt_from_monty_dev
+    _check(ctx.handle, fn(ctx.handle, field, ptr, n, stream), n)
 
 
 # -------------------------------------------------------- output layout ---

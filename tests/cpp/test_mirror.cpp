@@ -223,6 +223,32 @@ void check_server(const sfntt::Context& ctx) {
 
 }  // namespace
 
+// KoalaBear (no reference implementation): every variant and the coset LDE
+// against the oracle's KoalaBear restatement.
+void check_koalabear(const sfntt::Context& ctx) {
+  for (uint32_t log_n : {5u, 13u, 17u}) {
+    const size_t n = size_t(1) << log_n;
+    std::vector<uint32_t> x(n);
+    orc_lcg_fill(x.data(), n, 60 + log_n, ORC_KB_P, 2);
+    std::vector<uint32_t> ref = x;
+    orc_kb_forward(ref.data(), n);
+    sfntt::KbCudaCtGsR4 kb(ctx);
+    auto [y, ns] = kb.forward_ntt_gpu(x, log_n);
+    CHECK(y == ref, "KbCudaCtGsR4 forward log_n %u", log_n);
+    auto [z, ns2] = kb.inverse_ntt_gpu(y, log_n);
+    CHECK(z == x, "KbCudaCtGsR4 inverse(forward) log_n %u", log_n);
+    sfntt::KbCudaStockhamR2 st(ctx);
+    CHECK(st.forward_ntt_gpu(x, log_n).first == ref, "KbCudaStockhamR2 forward log_n %u", log_n);
+  }
+  const uint32_t log_n = 14, batch = 3, added = 2;
+  std::vector<uint32_t> x(size_t(batch) << log_n), ref(size_t(batch) << (log_n + added));
+  orc_lcg_fill(x.data(), x.size(), 91, ORC_KB_P, 2);
+  orc_kb_coset_lde(x.data(), ref.data(), log_n, batch, added, 0, 4);
+  for (bool fused : {true, false})
+    CHECK(sfntt::KbCosetLdeBatch(ctx, fused).execute(x, log_n, batch, added).data == ref,
+          "KbCosetLdeBatch %s log_n 14 batch 3 added 2", fused ? "fused" : "unfused");
+}
+
 int main(int argc, char** argv) {
   const bool no_device = argc > 1 && std::strcmp(argv[1], "--no-device") == 0;
   if (no_device) {
@@ -258,6 +284,7 @@ int main(int argc, char** argv) {
     check_backend<sfntt::BabyBear, sfntt::Variant::CtGsR4>(ctx);
     check_pointwise_and_batch(ctx);
     check_lde(ctx);
+    check_koalabear(ctx);
     check_layout(ctx);
     check_server(ctx);
   }

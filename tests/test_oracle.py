@@ -241,3 +241,94 @@ def test_reference_lde_shift_default():
     # lde/mod.rs:59, :158 -- shift = two_adic_generator(log_n_ext + 1)
     assert O.bb_from_monty(O.bb_two_adic_generator(22)) == 570250684
     assert O.bb_from_monty(O.bb_two_adic_generator(23)) == 1267047229
+
+
+# ---- KoalaBear (planned in the reference, README.md:20; no reference code) ---
+# The oracle runs the BabyBear code path over KoalaBear's constants, so the
+# BabyBear pins above cover the algorithm; these pin the constants and the
+# transforms against closed forms computed here in plain Python.
+KP = O.KB_P
+
+
+def _kb_from(a):
+    return [O.kb_from_monty(int(v)) for v in np.asarray(a).ravel()]
+
+
+def _kb_to(a):
+    return np.array([O.kb_to_monty(int(v)) for v in a], dtype=np.uint32)
+
+
+def _bitrev(k, bits):
+    return int(format(k, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def test_kb_constants():
+    assert KP == (1 << 31) - (1 << 24) + 1
+    assert (KP - 1) == (1 << 24) * 127
+    assert O.kb_to_monty(1) == (1 << 32) % KP
+    assert O.kb_to_monty(5) == (5 << 32) % KP
+    for v in (0, 1, 2, 12345, KP - 1):
+        assert O.kb_from_monty(O.kb_to_monty(v)) == v
+    rinv = pow(1 << 32, -1, KP)
+    for a, b in ((3, 5), (KP - 1, KP - 2), (1 << 30, 987654321)):
+        assert O.kb_mul(a, b) == a * b * rinv % KP
+    # 3 generates the multiplicative group: 3^((p-1)/q) != 1 for q in {2, 127}
+    assert pow(3, (KP - 1) // 2, KP) != 1 and pow(3, (KP - 1) // 127, KP) != 1
+
+
+@pytest.mark.parametrize("k", [0, 1, 2, 5, 13, 23, 24])
+def test_kb_two_adic_generator_order(k):
+    g = O.kb_from_monty(O.kb_two_adic_generator(k))
+    assert g == pow(3, (KP - 1) >> k, KP)
+    assert pow(g, 1 << k, KP) == 1
+    if k:
+        assert pow(g, 1 << (k - 1), KP) == KP - 1
+
+
+def _kb_naive_dft_bitrev(x):
+    n = len(x)
+    log_n = n.bit_length() - 1
+    w = pow(3, (KP - 1) >> log_n, KP)
+    nat = [sum(int(x[i]) * pow(w, i * k, KP) for i in range(n)) % KP for k in range(n)]
+    return [nat[_bitrev(k, log_n)] for k in range(n)]
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 5, 8, 10])
+def test_kb_forward_is_bitreversed_dft(log_n):
+    n = 1 << log_n
+    x = [(i * 7919 + 11) % KP for i in range(n)]
+    assert _kb_from(O.kb_forward(_kb_to(x))) == _kb_naive_dft_bitrev(x)
+    # inverse: bit-reversed evaluations back to coefficients, times n^-1 n
+    assert _kb_from(O.kb_inverse(_kb_to(_kb_naive_dft_bitrev(x)))) == x
+
+
+def test_kb_twiddles_and_batches():
+    tw, itw = O.kb_twiddles(6), O.kb_twiddles(6, inverse=True)
+    for s in range(6):
+        g = pow(3, (KP - 1) >> (s + 1), KP)
+        for j in range(1 << s):
+            assert O.kb_from_monty(int(tw[(1 << s) - 1 + j])) == pow(g, j, KP)
+            assert O.kb_from_monty(int(itw[(1 << s) - 1 + j])) == pow(g, KP - 1 - j, KP)
+    x = O.lcg(5 << 7, 77, KP, monty=True)
+    fw = O.kb_forward_batch(x, 7, 5, threads=3)
+    for c in range(5):
+        assert np.array_equal(fw[c << 7:(c + 1) << 7], O.kb_forward(x[c << 7:(c + 1) << 7]))
+    assert np.array_equal(O.kb_inverse_batch(fw, 7, 5), x)
+    with pytest.raises(O.InvalidSize):
+        O.kb_forward(np.zeros(1 << 25, dtype=np.uint32))
+
+
+@pytest.mark.parametrize("log_n,batch,added,shift", [(3, 2, 1, 0), (4, 1, 2, 0), (0, 3, 2, 0), (5, 2, 1, 3)])
+def test_kb_coset_lde_is_coset_evaluation(log_n, batch, added, shift):
+    n, ext = 1 << log_n, log_n + added
+    x = O.lcg(batch * n, 900 + log_n, KP, monty=True)
+    out = O.kb_coset_lde(x, log_n, batch, added, O.kb_to_monty(shift) if shift else 0)
+    g = shift or pow(3, (KP - 1) >> (ext + 1), KP)        # default: two_adic_generator(ext + 1)
+    w = pow(3, (KP - 1) >> ext, KP)
+    for c in range(batch):
+        coeffs = _kb_from(O.kb_inverse(x[c * n:(c + 1) * n]))   # bit-reversed evaluations -> coefficients
+        want = [sum(a * pow(g * pow(w, k, KP) % KP, i, KP) for i, a in enumerate(coeffs)) % KP
+                for k in range(1 << ext)]
+        got = _kb_from(out[c << ext:(c + 1) << ext])
+        assert got == [want[_bitrev(r, ext)] for r in range(1 << ext)], c
+    assert np.array_equal(out, O.kb_coset_lde(x, log_n, batch, added, O.kb_to_monty(shift) if shift else 0, threads=2))
