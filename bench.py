@@ -33,6 +33,7 @@ sys.path.insert(0, str(ROOT / "small-field-metal-ntt_b200"))
 sys.path.insert(0, str(ROOT))
 
 BB_P = 2013265921
+KB_P = 2130706433  # KoalaBear, 2^31 - 2^24 + 1
 METRIC = "BabyBear coset LDE 2^20x256 2x"
 PUBLISHED_MS = 821.0  # BASELINE.md / README.md:58 (Apple M3, Metal)
 
@@ -47,11 +48,12 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--added-bits", type=int, default=1)
     ap.add_argument("--mode", default="fused", choices=["fused", "unfused"])
-    ap.add_argument("--field", default="bb", choices=["bb", "m31"],
-                    help="bb: the BabyBear coset LDE (the headline); m31: the M31 blow-up of the same shape")
+    ap.add_argument("--field", default="bb", choices=["bb", "m31", "kb"],
+                    help="bb: the BabyBear coset LDE (the headline); m31: the M31 blow-up of the same shape; "
+                         "kb: the KoalaBear coset LDE of the same shape")
     ap.add_argument("--shift", default="31", choices=["31", "reference"],
-                    help="coset shift: g = 31 (the multiplicative generator) or the reference's default "
-                         "two_adic_generator(log_n_ext + 1); the cost is the same")
+                    help="coset shift: the multiplicative generator (31 for BabyBear, 3 for KoalaBear) or the "
+                         "reference's default two_adic_generator(log_n_ext + 1); the cost is the same")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -72,12 +74,16 @@ def shift_monty(a) -> int:
     """Montgomery form of the coset shift (0 = the reference default)."""
     if a.shift == "reference":
         return 0
+    if getattr(a, "field", "bb") == "kb":
+        return (3 << 32) % KB_P  # to_monty(3): KoalaBear's multiplicative generator
     return (31 << 32) % BB_P  # to_monty(31) = 31 * 2^32 mod p
 
 
 def metric_name(a) -> str:
     if a.field == "m31":
         return f"M31 blow-up 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
+    if a.field == "kb":
+        return f"KoalaBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
     return METRIC if (a.log_n, a.batch, a.added_bits) == (20, 256, 1) else \
         f"BabyBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
 
@@ -89,9 +95,10 @@ def workload(a) -> dict:
                 "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "layout": "SoA column-major, u32",
                 "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
                       f"{4 * a.batch << (a.log_n + a.added_bits) >> 20} MiB out per step)"}
-    return {"workload": f"BabyBear coset LDE 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x blow-up",
+    fname, g = ("KoalaBear", 3) if a.field == "kb" else ("BabyBear", 31)
+    return {"workload": f"{fname} coset LDE 2^{a.log_n} x {a.batch} cols, {1 << a.added_bits}x blow-up",
             "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
-            "shift": "g = 31, row i times 31^i" if a.shift == "31" else
+            "shift": f"g = {g}, row i times {g}^i" if a.shift == "31" else
                      "two_adic_generator(log_n_ext+1) (reference default)",
             "layout": "SoA column-major, Montgomery u32",
             "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
@@ -178,13 +185,20 @@ def ncu_traffic(kernel: str):
 
 # ------------------------------------------------------------ CPU legs ---
 def field_p(a) -> int:
-    return BB_P if a.field == "bb" else 2147483647
+    return {"bb": BB_P, "kb": KB_P}.get(a.field, 2147483647)
+
+
+def dtype_of(a) -> str:
+    return {"bb": "u32 (BabyBear Montgomery)", "kb": "u32 (KoalaBear Montgomery)"}.get(a.field, "u32 (M31 canonical)")
 
 
 def oracle_lde(a, O):
     """The oracle's LDE of the bench's field: f(x, columns, threads)."""
     if a.field == "m31":
         return lambda x, cols, threads: O.m31_lde(x, a.log_n, cols, a.added_bits, threads=threads)
+    if a.field == "kb":
+        return lambda x, cols, threads: O.kb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a),
+                                                       threads=threads)
     return lambda x, cols, threads: O.bb_coset_lde(x, a.log_n, cols, a.added_bits, shift_monty=shift_monty(a),
                                                    threads=threads)
 
@@ -196,13 +210,13 @@ def cpu_lde_sample(a, target_s: float) -> dict:
     threads = O.default_threads()
     n = 1 << a.log_n
     lde = oracle_lde(a, O)
-    one = O.lcg(n, 1, field_p(a), monty=a.field == "bb")
+    one = O.lcg(n, 1, field_p(a), monty=a.field != "m31")
     t = time.perf_counter()
     lde(one, 1, 1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(target_s * threads / max(t1, 1e-6)))))
     cols = max(1, min(a.batch, (cols // threads) * threads or cols))
-    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field == "bb")
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field != "m31")
     t = time.perf_counter()
     lde(x, cols, threads)
     ts = time.perf_counter() - t
@@ -221,10 +235,10 @@ def run_reference(a, rank: int) -> None:
     per_step = max(0.3, min(20.0, 150.0 / max(1, a.steps + a.warmup)))  # whole run ~2.5 min
     lde = oracle_lde(a, O)
     t = time.perf_counter()
-    lde(O.lcg(n, 1, field_p(a), monty=a.field == "bb"), 1, 1)
+    lde(O.lcg(n, 1, field_p(a), monty=a.field != "m31"), 1, 1)
     t1 = time.perf_counter() - t
     cols = int(max(1, min(a.batch, round(per_step * threads / max(t1, 1e-6)))))
-    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field == "bb")
+    x = O.lcg(cols << a.log_n, 42 + a.log_n, field_p(a), monty=a.field != "m31")
     times = []
     for i in range(a.warmup + a.steps):
         t = time.perf_counter()
@@ -236,7 +250,7 @@ def run_reference(a, rank: int) -> None:
     line = {"impl": "reference", "metric": metric_name(a), "value": ms, "unit": "ms", "n_gpus": a.gpus,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": ms / PUBLISHED_MS if metric_name(a) == METRIC else None,
-            "dtype": "u32 (BabyBear Montgomery)" if a.field == "bb" else "u32 (M31 canonical)", "data": "synthetic",
+            "dtype": dtype_of(a), "data": "synthetic",
             "config": workload(a),
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -286,9 +300,10 @@ def main() -> None:
         def host_call(hin, hout):
             lde.execute(hin, a.log_n, a.batch, a.added_bits, out=hout)
     else:
-        lde = sfntt.CosetLdeBatch(ctx, fused=(a.mode == "fused"))
-        sfntt._check(ctx.handle, sfntt._ffi.lib().sfntt_bb_to_monty_dev(ctx.handle, x.data_ptr(), x.numel(), stream))
-        ctx.prepare_lde(sfntt.FIELD_BABYBEAR, a.log_n, a.added_bits, shift)
+        fid = sfntt.FIELD_KOALABEAR if a.field == "kb" else sfntt.FIELD_BABYBEAR
+        lde = (sfntt.KbCosetLdeBatch if a.field == "kb" else sfntt.CosetLdeBatch)(ctx, fused=(a.mode == "fused"))
+        sfntt.convert_monty_dev(ctx, fid, x.data_ptr(), x.numel(), to_monty=True, stream=stream)
+        ctx.prepare_lde(fid, a.log_n, a.added_bits, shift)
 
         def step():
             lde.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, shift_monty=shift,
@@ -394,7 +409,7 @@ def main() -> None:
     line = {"metric": metric_name(a), "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": value / PUBLISHED_MS if metric_name(a) == METRIC else None,
-            "dtype": "u32 (M31 canonical, exact)" if m31 else "u32 (BabyBear Montgomery, exact)",
+            "dtype": dtype_of(a)[:-1] + ", exact)",
             "data": "synthetic: seeded uniform canonical values in [0, p)" + ("" if m31 else ", Montgomery on device"),
             "config": {**workload(a), "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "gpu_launches": launches, "launches_per_step": launches / a.steps,
@@ -448,6 +463,11 @@ def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
     ctx.prepare_lde(sfntt.FIELD_M31, a.log_n, a.added_bits)
     res["m31_lde_ms"] = timed(lambda: m31.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits,
                                                       stream=stream))
+    # the KoalaBear coset LDE of the same shape (words < BabyBear p are valid KoalaBear Montgomery words)
+    kb = sfntt.KbCosetLdeBatch(ctx)
+    ctx.prepare_lde(sfntt.FIELD_KOALABEAR, a.log_n, a.added_bits)
+    res["kb_lde_ms"] = timed(lambda: kb.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits,
+                                                    stream=stream))
     del rows
     return res
 
@@ -723,8 +743,8 @@ def kernel_butterflies(name: str, bytes_per_launch: int, added_bits: int) -> flo
 
 def secondary_metrics(ctx, sfntt, torch) -> dict:
     """The single-column NTT configurations: BabyBear forward + inverse for
-    log n = 10..24 and the M31 Circle NTT likewise (n = 2^16 is the M31
-    configuration), values uniform in [0, p), device-resident; 10 forward +
+    log n = 10..24, the M31 Circle NTT and the KoalaBear NTT likewise (n = 2^16
+    is the M31 configuration), values uniform in [0, p), device-resident; 10 forward +
     inverse pairs captured in a CUDA graph, replayed 10 times after 5 warm-up
     pairs, so small sizes measure the device rather than the host's launch rate.  Columns up to 2^24 words (64 MiB) stay resident in
     the 126 MB L2 across repetitions, so the byte fraction is against HBM
@@ -733,11 +753,15 @@ def secondary_metrics(ctx, sfntt, torch) -> dict:
                    "replayed from a CUDA graph"}
     stream = torch.cuda.current_stream().cuda_stream
     peak, _ = peaks()
-    for field, name in ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31")):
-        b = (sfntt.BbCudaCtGsR4 if field == sfntt.FIELD_BABYBEAR else sfntt.CudaCtGsR4)(ctx)
+    backends = {sfntt.FIELD_BABYBEAR: sfntt.BbCudaCtGsR4, sfntt.FIELD_M31: sfntt.CudaCtGsR4,
+                sfntt.FIELD_KOALABEAR: sfntt.KbCudaCtGsR4}
+    primes = {sfntt.FIELD_BABYBEAR: BB_P, sfntt.FIELD_M31: 2147483647, sfntt.FIELD_KOALABEAR: KB_P}
+    fields = ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31"), (sfntt.FIELD_KOALABEAR, "kb"))
+    for field, name in fields:
+        b = backends[field](ctx)
         rows = {}
         for log_n in range(10, 25):
-            p = BB_P if field == sfntt.FIELD_BABYBEAR else 2147483647
+            p = primes[field]
             d = torch.randint(0, p, (1 << log_n,), dtype=torch.int64, device="cuda").to(torch.int32)
             ctx.prepare(field, log_n)
             for _ in range(5):
@@ -770,8 +794,8 @@ def secondary_metrics(ctx, sfntt, torch) -> dict:
     res["m31_2^16_fwd_inv_us"] = res["m31"]["16"]["fwd_inv_us"]
     # many small columns (lattice-crypto shapes): 2^24 points per batch
     lattice = {}
-    for field, name in ((sfntt.FIELD_BABYBEAR, "bb"), (sfntt.FIELD_M31, "m31")):
-        b = (sfntt.BbCudaCtGsR4 if field == sfntt.FIELD_BABYBEAR else sfntt.CudaCtGsR4)(ctx)
+    for field, name in fields:
+        b = backends[field](ctx)
         for log_n in (8, 10):
             cols = 1 << (24 - log_n)
             d = torch.randint(0, BB_P, (cols << log_n,), dtype=torch.int64, device="cuda").to(torch.int32)
