@@ -181,6 +181,23 @@ int sfntt_bb_from_monty_dev(sfntt_ctx *ctx, uint32_t *d_data, size_t len, void *
 int sfntt_to_monty_dev(sfntt_ctx *ctx, int field, uint32_t *d_data, size_t len, void *stream);
 int sfntt_from_monty_dev(sfntt_ctx *ctx, int field, uint32_t *d_data, size_t len, void *stream);
 
+/* ---- M31 quadratic extension CM31 = M31[i]/(i^2 + 1) (planned in the
+ * reference, TODOS.md:27-31).  An element is an interleaved pair (re, im) of
+ * canonical M31 words; a batch is `batch` columns of 2^log_n pairs
+ * (len = 2 * (batch << log_n) words).  The Circle NTT of a CM31 column is the
+ * Circle NTT of its real parts plus i times that of its imaginary parts (the
+ * twiddles lie in M31), with the M31 conventions (forward: bit-reversed out;
+ * inverse: times n^-1).  The device calls use a context scratch of
+ * 8 * (batch << log_n) bytes: call sfntt_cm31_prepare before a graph capture. */
+int sfntt_cm31_prepare(sfntt_ctx *ctx, uint32_t log_n, uint32_t batch);
+int sfntt_cm31_ntt_dev(sfntt_ctx *ctx, int inverse, uint32_t *d_pairs, uint32_t log_n, uint32_t batch,
+                       void *stream);
+int sfntt_cm31_ntt(sfntt_ctx *ctx, int inverse, const uint32_t *in, size_t len, uint32_t log_n,
+                   uint32_t batch, uint32_t *out, uint64_t *gpu_ns);
+/* out[k] = a[k] * b[k] in CM31 for n pairs (8-byte aligned device pointers). */
+int sfntt_cm31_mul_dev(sfntt_ctx *ctx, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out, size_t n,
+                       void *stream);
+
 /* ---- Uneven batches in one graph launch (no reference counterpart: the
  * north-star batching pattern).  An item is `batch` SoA columns of 2^log_n
  * points of any field, extended by 2^added_bits: BabyBear items are the

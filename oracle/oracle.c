@@ -515,6 +515,41 @@ int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batc
     return 0;
 }
 
+/* ================= CM31 = M31[i] / (i^2 + 1) (TODOS.md:27-31) ============ */
+
+/* Not implemented in the reference (planned).  (a + bi)(c + di) =
+ * (ac - bd) + (ad + bc) i over M31; a transform of CM31 columns with M31
+ * twiddles is the M31 transform of each coordinate. */
+void orc_cm31_mul(const uint32_t *a, const uint32_t *b, uint32_t *out, size_t n)
+{
+    for (size_t k = 0; k < n; k++) {
+        uint32_t ar = a[2 * k], ai = a[2 * k + 1], br = b[2 * k], bi = b[2 * k + 1];
+        uint32_t re = orc_m31_sub(orc_m31_mul(ar, br), orc_m31_mul(ai, bi));
+        uint32_t im = orc_m31_add(orc_m31_mul(ar, bi), orc_m31_mul(ai, br));
+        out[2 * k] = re;
+        out[2 * k + 1] = im;
+    }
+}
+
+int orc_cm31_ntt(uint32_t *pairs, uint32_t log_n, uint32_t batch, int inverse)
+{
+    if (log_n > 30) return 1;
+    if (log_n == 0) return 0;
+    size_t n = (size_t)1 << log_n;
+    uint32_t *col = (uint32_t *)malloc(n * sizeof(uint32_t));
+    for (uint32_t c = 0; c < batch; c++) {
+        uint32_t *p = pairs + 2 * (size_t)c * n;
+        for (int part = 0; part < 2; part++) {
+            for (size_t j = 0; j < n; j++) col[j] = p[2 * j + part];
+            if (inverse) orc_m31_inverse(col, n);
+            else orc_m31_forward(col, n);
+            for (size_t j = 0; j < n; j++) p[2 * j + part] = col[j];
+        }
+    }
+    free(col);
+    return 0;
+}
+
 /* ============================ Data generator ============================= */
 
 uint64_t orc_lcg_fill(uint32_t *out, size_t n, uint64_t seed, uint32_t p, int monty)

@@ -115,6 +115,12 @@ int orc_kb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
                      uint32_t batch, uint32_t added_bits, uint32_t shift_monty,
                      int threads);
 
+/* ---- CM31 = M31[i]/(i^2+1): interleaved (re, im) pairs (not in the
+ * reference; TODOS.md:27-31 plans it).  orc_cm31_ntt transforms `batch`
+ * columns of 2^log_n pairs in place with the M31 NTT on each coordinate. */
+void orc_cm31_mul(const uint32_t *a, const uint32_t *b, uint32_t *out, size_t n);
+int orc_cm31_ntt(uint32_t *pairs, uint32_t log_n, uint32_t batch, int inverse);
+
 /* Reference data generator (src/ntt/test_utils.rs:38-46, benches seeds):
  * s = s*6364136223846793005 + 1; v = (s >> 33) % p.  BabyBear to_monty
  * applied when monty == 1, KoalaBear's when monty == 2.  Returns the final

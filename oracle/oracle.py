@@ -73,6 +73,8 @@ def lib():
             "orc_bb_forward_batch": (i, [_u32p, u32, u32, i]),
             "orc_bb_inverse_batch": (i, [_u32p, u32, u32, i]),
             "orc_lcg_fill": (u64, [_u32p, sz, u64, u32, i]),
+            "orc_cm31_mul": (None, [_u32p, _u32p, _u32p, sz]),
+            "orc_cm31_ntt": (i, [_u32p, u32, u32, i]),
             "orc_kb_to_monty": (u32, [u32]),
             "orc_kb_from_monty": (u32, [u32]),
             "orc_kb_mul": (u32, [u32, u32]),
@@ -223,6 +225,25 @@ def m31_lde(data, log_n: int, batch: int, added_bits: int, threads: int = 1) -> 
     if lib().orc_m31_lde(_ptr(a), _ptr(out), log_n, batch, added_bits, threads) != 0:
         raise InvalidSize(a.size)
     return out
+
+
+def cm31_mul(a, b) -> np.ndarray:
+    """CM31 products of interleaved (re, im) pairs."""
+    a_, b_ = _arr(a), _arr(b)
+    assert a_.size == b_.size and a_.size % 2 == 0
+    out = np.empty_like(a_)
+    lib().orc_cm31_mul(_ptr(a_), _ptr(b_), _ptr(out), a_.size // 2)
+    return out
+
+
+def cm31_ntt(pairs, log_n: int, batch: int, inverse: bool = False) -> np.ndarray:
+    """Circle NTT of `batch` CM31 columns of 2^log_n interleaved pairs."""
+    a = _arr(pairs).copy()
+    if a.size != 2 * (batch << log_n):
+        raise InvalidSize(a.size)
+    if lib().orc_cm31_ntt(_ptr(a), log_n, batch, int(inverse)) != 0:
+        raise InvalidSize(a.size)
+    return a
 
 
 def lcg(n: int, seed: int, p: int, monty: bool = False) -> np.ndarray:

@@ -274,6 +274,7 @@ void sfntt_ctx_destroy(sfntt_ctx* ctx) {
     ctx->buf_in.release();
     ctx->buf_out.release();
     ctx->buf_aux.release();
+    ctx->buf_ext.release();
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
     for (cudaStream_t s : ctx->copy_streams)
@@ -542,6 +543,63 @@ int sfntt_from_monty_dev(sfntt_ctx* ctx, int field, uint32_t* d, size_t len, voi
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
   return finish(ctx, sfntt::monty_convert_dev(ctx, field, false, d, len, (cudaStream_t)stream));
+}
+
+int sfntt_cm31_prepare(sfntt_ctx* ctx, uint32_t log_n, uint32_t batch) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  Status s = check_log(SFNTT_M31, log_n);
+  if (s.ok() && log_n > 0) {
+    const uint2* tw;
+    for (int inv = 0; inv < 2 && s.ok(); ++inv) s = sfntt::m31_twiddles(ctx, inv, log_n, ctx->stream, &tw);
+    uint32_t* scratch = nullptr;
+    if (s.ok()) s = sfntt::cm31_scratch(ctx, log_n, batch, ctx->stream, &scratch);
+  }
+  return finish(ctx, s);
+}
+
+int sfntt_cm31_ntt_dev(sfntt_ctx* ctx, int inverse, uint32_t* d_pairs, uint32_t log_n, uint32_t batch, void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::cm31_ntt_dev(ctx, inverse != 0, d_pairs, log_n, batch, (cudaStream_t)stream));
+}
+
+int sfntt_cm31_ntt(sfntt_ctx* ctx, int inverse, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
+                   uint32_t* out, uint64_t* gpu_ns) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  if (gpu_ns) *gpu_ns = 0;
+  Status s = check_log(SFNTT_M31, log_n);
+  if (s.ok() && len != ((size_t)batch << log_n) * 2)
+    s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != 2 * (batch << log_n)"};
+  if (s.ok() && len && (!in || !out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  if (s.ok() && len) {
+    s = [&]() -> Status {
+      const size_t bytes = len * sizeof(uint32_t);
+      SFNTT_TRY(ctx->buf_in.reserve(bytes));
+      uint32_t* d = ctx->buf_in.as<uint32_t>();
+      SFNTT_CU(cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_start, ctx->stream));
+      SFNTT_TRY(sfntt::cm31_ntt_dev(ctx, inverse != 0, d, log_n, batch, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_stop, ctx->stream));
+      SFNTT_CU(cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      SFNTT_CU(cudaStreamSynchronize(ctx->stream));
+      SFNTT_TRY(device_flag(ctx));
+      return elapsed_ns(ctx, gpu_ns);
+    }();
+  }
+  return finish(ctx, s);
+}
+
+int sfntt_cm31_mul_dev(sfntt_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_out, size_t n,
+                       void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::cm31_mul_dev(ctx, d_a, d_b, d_out, n, (cudaStream_t)stream));
 }
 
 int sfntt_host_alloc(sfntt_ctx* ctx, size_t bytes, void** out) {

@@ -106,6 +106,8 @@ struct sfntt_ctx {
 
   // staging for host-memory calls
   sfntt::DevBuf buf_in, buf_out, buf_aux;
+  // base-field planes of CM31 transforms (ext.cu)
+  sfntt::DevBuf buf_ext;
   // device int set by a kernel whose bounded wait ran out (SFNTT_TIMEOUT)
   sfntt::DevBuf err;
   // route every pass through the first (non-TMA) tile engine (tests / A-B)
@@ -182,6 +184,10 @@ Status layout_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t lo
 // One LDE / blow-up work item (batch.cu): run under its plan, or make its tables resident.
 Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
 Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s);
+// CM31 = M31[i]/(i^2+1), interleaved (re, im) pairs (ext.cu).
+Status cm31_scratch(sfntt_ctx* ctx, uint32_t log_n, uint32_t batch, cudaStream_t s, uint32_t** out);
+Status cm31_ntt_dev(sfntt_ctx* ctx, bool inverse, uint32_t* d_pairs, uint32_t log_n, uint32_t batch, cudaStream_t s);
+Status cm31_mul_dev(sfntt_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t* out, size_t n, cudaStream_t s);
 Status pointwise_mul_dev(sfntt_ctx* ctx, int field, const uint32_t* a, const uint32_t* b, uint32_t* out,
                          size_t n, cudaStream_t stream);
 Status monty_convert_dev(sfntt_ctx* ctx, int field, bool to_monty, uint32_t* d, size_t n, cudaStream_t stream);

@@ -441,6 +441,44 @@ class M31Lde:
         _check(self.ctx.handle, st, batch_size << log_n)
 
 
+class Cm31Ntt:
+    """Circle NTT over the M31 quadratic extension CM31 = M31[i]/(i^2+1)
+    (planned in the reference, TODOS.md:27-31): `batch` columns of 2^log_n
+    interleaved (re, im) pairs of canonical M31 words; the M31 transform of
+    each coordinate (the twiddles lie in M31)."""
+
+    def __init__(self, ctx: Context | None = None, device: int = 0):
+        self.ctx = ctx or default_context(device)
+
+    def _host(self, inverse: bool, pairs, log_n: int, batch: int):
+        inp = _u32(pairs)
+        out = np.empty_like(inp)
+        ns = ctypes.c_uint64()
+        st = _ffi.lib().sfntt_cm31_ntt(self.ctx.handle, int(inverse), _p(inp), inp.size, log_n, batch, _p(out),
+                                       ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return out, int(ns.value)
+
+    def forward_batch_gpu(self, pairs, log_n: int, batch: int = 1):
+        return self._host(False, pairs, log_n, batch)
+
+    def inverse_batch_gpu(self, pairs, log_n: int, batch: int = 1):
+        return self._host(True, pairs, log_n, batch)
+
+    def prepare(self, log_n: int, batch: int) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_cm31_prepare(self.ctx.handle, log_n, batch))
+
+    def forward_dev(self, ptr: int, log_n: int, batch: int = 1, stream: int = 0) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_cm31_ntt_dev(self.ctx.handle, 0, ptr, log_n, batch, stream))
+
+    def inverse_dev(self, ptr: int, log_n: int, batch: int = 1, stream: int = 0) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_cm31_ntt_dev(self.ctx.handle, 1, ptr, log_n, batch, stream))
+
+    def mul_dev(self, a_ptr: int, b_ptr: int, out_ptr: int, n: int, stream: int = 0) -> None:
+        """out[k] = a[k] * b[k] for n CM31 pairs."""
+        _check(self.ctx.handle, _ffi.lib().sfntt_cm31_mul_dev(self.ctx.handle, a_ptr, b_ptr, out_ptr, n, stream))
+
+
 def convert_monty_dev(ctx: Context, field: int, ptr: int, n: int, to_monty: bool, stream: int = 0) -> None:
     """In-place canonical <-> Montgomery conversion of n device words
     (BabyBear::to_monty / from_monty, src/field/babybear.rs:54-65; KoalaBear alike)."""

@@ -332,3 +332,36 @@ def test_kb_coset_lde_is_coset_evaluation(log_n, batch, added, shift):
         got = _kb_from(out[c << ext:(c + 1) << ext])
         assert got == [want[_bitrev(r, ext)] for r in range(1 << ext)], c
     assert np.array_equal(out, O.kb_coset_lde(x, log_n, batch, added, O.kb_to_monty(shift) if shift else 0, threads=2))
+
+
+# ---- CM31 = M31[i] / (i^2 + 1) (planned in the reference, TODOS.md:27-31) ----
+def test_cm31_mul_is_complex_product():
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, MP, 2 * 64, dtype=np.uint64).astype(np.uint32)
+    b = rng.integers(0, MP, 2 * 64, dtype=np.uint64).astype(np.uint32)
+    got = O.cm31_mul(a, b)
+    for k in range(64):
+        ar, ai, br, bi = (int(a[2 * k]), int(a[2 * k + 1]), int(b[2 * k]), int(b[2 * k + 1]))
+        assert int(got[2 * k]) == (ar * br - ai * bi) % MP
+        assert int(got[2 * k + 1]) == (ar * bi + ai * br) % MP
+    i = np.array([0, 1], np.uint32)
+    assert list(O.cm31_mul(i, i)) == [MP - 1, 0]  # i^2 = -1
+
+
+def test_cm31_ntt_is_componentwise():
+    log_n, batch = 6, 3
+    re = O.lcg(batch << log_n, 5, MP)
+    im = O.lcg(batch << log_n, 6, MP)
+    pairs = np.empty(2 * re.size, np.uint32)
+    pairs[0::2], pairs[1::2] = re, im
+    fw = O.cm31_ntt(pairs, log_n, batch)
+    n = 1 << log_n
+    for c in range(batch):
+        col = fw[2 * c * n:2 * (c + 1) * n]
+        assert np.array_equal(col[0::2], O.m31_forward(re[c * n:(c + 1) * n]))
+        assert np.array_equal(col[1::2], O.m31_forward(im[c * n:(c + 1) * n]))
+    assert np.array_equal(O.cm31_ntt(fw, log_n, batch, inverse=True), pairs)
+    # C-linearity: transform(i * x) = i * transform(x)
+    i_pairs = O.cm31_mul(np.tile(np.array([0, 1], np.uint32), re.size), pairs)
+    assert np.array_equal(O.cm31_ntt(i_pairs, log_n, batch),
+                          O.cm31_mul(np.tile(np.array([0, 1], np.uint32), re.size), fw))
