@@ -463,6 +463,11 @@ def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
     ctx.prepare_lde(sfntt.FIELD_M31, a.log_n, a.added_bits)
     res["m31_lde_ms"] = timed(lambda: m31.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits,
                                                       stream=stream))
+    # the canonic-coset circle LDE of the same shape (M31 network, circle-FFT twiddles)
+    circ = sfntt.CircleLde(ctx)
+    circ.prepare(a.log_n, a.added_bits)
+    res["circle_lde_ms"] = timed(lambda: circ.execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch,
+                                                          a.added_bits, stream=stream))
     # the KoalaBear coset LDE of the same shape (words < BabyBear p are valid KoalaBear Montgomery words)
     kb = sfntt.KbCosetLdeBatch(ctx)
     ctx.prepare_lde(sfntt.FIELD_KOALABEAR, a.log_n, a.added_bits)

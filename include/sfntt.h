@@ -134,6 +134,28 @@ int sfntt_coset_lde(sfntt_ctx *ctx, int field, const uint32_t *in, size_t len, u
 int sfntt_m31_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n,
                   uint32_t batch, uint32_t added_bits, uint32_t *out, uint64_t *gpu_ns);
 
+/* ---- Canonic-coset circle FFT and circle LDE over M31 (Stwo-style; the
+ * reference lists an M31 circle LDE as a goal without code).  Domain
+ * odds(log_n) = G_{2^(log_n+1)} + <G_{2^log_n}> ordered as the half coset
+ * h_i = (1 + 4i) G_{2^(log_n+1)}, i < n/2, then its conjugates; values in
+ * bit-reversed order of that domain; coefficient r multiplies
+ * y^{r_0} x^{r_1} pi(x)^{r_2} pi^2(x)^{r_3} ... with pi(x) = 2x^2 - 1, so the
+ * LDE (interpolate -> zero-pad -> evaluate on odds(log_n + added_bits)) is a
+ * genuine low-degree extension.  The butterfly network and data conventions
+ * are the reference's M31 ones (src/ntt/m31/cpu_reference.rs:50-120); only
+ * the twiddles differ: layer 0 uses y(h), layer L >= 1 x(2^(L-1) h).
+ * sfntt_circle_ntt: inverse = 0 evaluates coefficients, 1 interpolates
+ * (times n^-1); len = batch << log_n. */
+int sfntt_circle_ntt(sfntt_ctx *ctx, int inverse, const uint32_t *in, size_t len, uint32_t log_n,
+                     uint32_t batch, uint32_t *out, uint64_t *gpu_ns);
+int sfntt_circle_lde(sfntt_ctx *ctx, const uint32_t *in, size_t len, uint32_t log_n, uint32_t batch,
+                     uint32_t added_bits, uint32_t *out, uint64_t *gpu_ns);
+int sfntt_prepare_circle(sfntt_ctx *ctx, uint32_t log_n, uint32_t added_bits);
+int sfntt_circle_ntt_dev(sfntt_ctx *ctx, int inverse, uint32_t *d_data, uint32_t log_n, uint32_t batch,
+                         void *stream);
+int sfntt_circle_lde_dev(sfntt_ctx *ctx, const uint32_t *d_in, uint32_t *d_out, uint32_t log_n,
+                         uint32_t batch, uint32_t added_bits, void *stream);
+
 /* ---- device-pointer twins (stream = cudaStream_t; NULL = legacy default).
  * Asynchronous; no host synchronisation and no allocation when the tables
  * for (field, log_n) are cached. */

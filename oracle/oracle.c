@@ -515,6 +515,91 @@ int orc_m31_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batc
     return 0;
 }
 
+/* ============ Canonic-coset circle FFT and circle LDE (Stwo-style) ======== */
+
+/* Not in the reference, which lists "M31 Circle LDE proper" only as a goal
+ * and comments Stwo out (tests/ntt_cross_validation.rs:281-298).  Definition
+ * (the circle FFT of the Circle STARKs construction, restated here):
+ *   domain D_k = odds(k) in the order D[i] = h_i (i < n/2), D[n/2 + i] =
+ *   conj(h_i), h_i = G_{2^(k+1)} + i G_{2^(k-1)}; values in bit-reversed order
+ *   (storage r holds f(D[bitrev_k(r)])); coefficient r multiplies the basis
+ *   y^{r_0} x^{r_1} pi(x)^{r_2} pi^2(x)^{r_3} ... (pi(x) = 2x^2 - 1), so
+ *   padding coefficients with zeros keeps the function.
+ * The network is the reference's M31 network (m31/cpu_reference.rs:61-107:
+ * per-block twiddles, layer L stride 2^L) with these twiddles:
+ *   T_0[b] = y(h_{bitrev_{k-1}(b)}),  T_L[b] = x(2^{L-1} h_{bitrev_{k-1-L}(b)}) (L >= 1).
+ * Every twiddle is a coordinate of m G_{2^(k+1)}: h_i = (1 + 4i) G_{2^(k+1)}. */
+static orc_cpoint gpow(uint32_t k, uint64_t m) /* m G_{2^(k+1)}, m mod 2^(k+1) */
+{
+    return orc_circle_mul_scalar(orc_circle_subgroup_gen(k + 1), (uint32_t)(m & (((uint64_t)1 << (k + 1)) - 1)));
+}
+
+void orc_circle_twiddles(uint32_t log_n, int inverse, uint32_t *out)
+{
+    size_t n = (size_t)1 << log_n;
+    for (uint32_t L = 0; L < log_n; L++) {
+        size_t cnt = n >> (L + 1);
+        uint32_t *dst = out + (n - (n >> L));
+        uint32_t bits = log_n - 1 - L;
+        for (size_t b = 0; b < cnt; b++) {
+            uint64_t i = bit_reverse_idx(b, bits);
+            uint64_t m = (1 + 4 * i) << (L ? L - 1 : 0);
+            orc_cpoint p = gpow(log_n, m);
+            uint32_t t = L == 0 ? p.y : p.x;
+            dst[b] = inverse ? orc_m31_inv(t) : t;
+        }
+    }
+}
+
+static uint32_t *g_ctw_cache[2][32];
+
+static const uint32_t *ctw_get(int inverse, uint32_t log_n)
+{
+    uint32_t **slot = &g_ctw_cache[inverse][log_n];
+    if (*slot == NULL) {
+        uint32_t *t = (uint32_t *)malloc(((size_t)1 << log_n) * sizeof(uint32_t));
+        orc_circle_twiddles(log_n, inverse, t);
+        *slot = t;
+    }
+    return *slot;
+}
+
+int orc_circle_ntt(uint32_t *data, uint32_t log_n, uint32_t batch, int inverse)
+{
+    if (log_n > 30) return 1;
+    if (log_n == 0) return 0;
+    size_t n = (size_t)1 << log_n;
+    const uint32_t *tw = ctw_get(inverse, log_n);
+    for (uint32_t c = 0; c < batch; c++) {
+        if (inverse) m31_inverse_tw(data + (size_t)c * n, n, log_n, tw);
+        else m31_forward_tw(data + (size_t)c * n, n, log_n, tw);
+    }
+    return 0;
+}
+
+/* Interpolate on D_{log_n} (values bit-reversed), zero-pad the coefficients,
+ * evaluate on D_{log_n + added_bits}. */
+int orc_circle_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                   uint32_t added_bits, int threads)
+{
+    uint32_t log_n_ext = log_n + added_bits;
+    if (log_n_ext > 30) return 1;
+    size_t n = (size_t)1 << log_n, n_ext = (size_t)1 << log_n_ext;
+    const uint32_t *itw = log_n ? ctw_get(1, log_n) : NULL;
+    const uint32_t *tw = log_n_ext ? ctw_get(0, log_n_ext) : NULL;
+    long c;
+    (void)threads;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(clamp_threads(threads))
+    for (c = 0; c < (long)batch; c++) {
+        uint32_t *dst = out + (size_t)c * n_ext;
+        memcpy(dst, in + (size_t)c * n, n * sizeof(uint32_t));
+        if (log_n) m31_inverse_tw(dst, n, log_n, itw);
+        memset(dst + n, 0, (n_ext - n) * sizeof(uint32_t));
+        if (log_n_ext) m31_forward_tw(dst, n_ext, log_n_ext, tw);
+    }
+    return 0;
+}
+
 /* ================= CM31 = M31[i] / (i^2 + 1) (TODOS.md:27-31) ============ */
 
 /* Not implemented in the reference (planned).  (a + bi)(c + di) =

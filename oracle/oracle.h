@@ -115,6 +115,16 @@ int orc_kb_coset_lde(const uint32_t *in, uint32_t *out, uint32_t log_n,
                      uint32_t batch, uint32_t added_bits, uint32_t shift_monty,
                      int threads);
 
+/* ---- Canonic-coset circle FFT and circle LDE (Stwo-style; not in the
+ * reference).  Domain odds(log_n) ordered half coset then conjugates, values
+ * bit-reversed, coefficient r on the basis y^{r_0} x^{r_1} pi(x)^{r_2} ...;
+ * the reference's M31 network with twiddles T_0[b] = y(h_{rev(b)}),
+ * T_L[b] = x(2^{L-1} h_{rev(b)}).  Layout of the twiddles as orc_m31_twiddles. */
+void orc_circle_twiddles(uint32_t log_n, int inverse, uint32_t *out);
+int orc_circle_ntt(uint32_t *data, uint32_t log_n, uint32_t batch, int inverse);
+int orc_circle_lde(const uint32_t *in, uint32_t *out, uint32_t log_n, uint32_t batch,
+                   uint32_t added_bits, int threads);
+
 /* ---- CM31 = M31[i]/(i^2+1): interleaved (re, im) pairs (not in the
  * reference; TODOS.md:27-31 plans it).  orc_cm31_ntt transforms `batch`
  * columns of 2^log_n pairs in place with the M31 NTT on each coordinate. */

@@ -73,6 +73,9 @@ def lib():
             "orc_bb_forward_batch": (i, [_u32p, u32, u32, i]),
             "orc_bb_inverse_batch": (i, [_u32p, u32, u32, i]),
             "orc_lcg_fill": (u64, [_u32p, sz, u64, u32, i]),
+            "orc_circle_twiddles": (None, [u32, i, _u32p]),
+            "orc_circle_ntt": (i, [_u32p, u32, u32, i]),
+            "orc_circle_lde": (i, [_u32p, _u32p, u32, u32, u32, i]),
             "orc_cm31_mul": (None, [_u32p, _u32p, _u32p, sz]),
             "orc_cm31_ntt": (i, [_u32p, u32, u32, i]),
             "orc_kb_to_monty": (u32, [u32]),
@@ -223,6 +226,31 @@ def m31_lde(data, log_n: int, batch: int, added_bits: int, threads: int = 1) -> 
         raise InvalidSize(a.size)
     out = np.empty(batch << (log_n + added_bits), dtype=np.uint32)
     if lib().orc_m31_lde(_ptr(a), _ptr(out), log_n, batch, added_bits, threads) != 0:
+        raise InvalidSize(a.size)
+    return out
+
+
+def circle_twiddles(log_n: int, inverse: bool = False) -> np.ndarray:
+    out = np.zeros(max((1 << log_n) - 1, 1), dtype=np.uint32)
+    lib().orc_circle_twiddles(log_n, int(inverse), _ptr(out))
+    return out[: (1 << log_n) - 1]
+
+
+def circle_ntt(data, log_n: int, batch: int = 1, inverse: bool = False) -> np.ndarray:
+    """Canonic-coset circle FFT (evaluate) / its inverse (interpolate, times n^-1)."""
+    a = _arr(data).copy()
+    if a.size != batch << log_n or lib().orc_circle_ntt(_ptr(a) if a.size else None, log_n, batch,
+                                                           int(inverse)) != 0:
+        raise InvalidSize(a.size)
+    return a
+
+
+def circle_lde(data, log_n: int, batch: int, added_bits: int, threads: int = 1) -> np.ndarray:
+    a = _arr(data)
+    if a.size != batch << log_n:
+        raise InvalidSize(a.size)
+    out = np.empty(batch << (log_n + added_bits), dtype=np.uint32)
+    if lib().orc_circle_lde(_ptr(a), _ptr(out), log_n, batch, added_bits, threads) != 0:
         raise InvalidSize(a.size)
     return out
 

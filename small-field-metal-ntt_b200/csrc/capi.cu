@@ -46,6 +46,9 @@ int finish(sfntt_ctx* ctx, const Status& s) {
 bool is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
 uint32_t ilog2(size_t n) { uint32_t l = 0; while (((size_t)1 << l) < n) ++l; return l; }
 
+// Internal LDE mode of M31 host calls: the canonic-coset circle LDE.
+constexpr int kCircleLde = 1 << 8;
+
 Status check_field(int field) {
   if (!sfntt::valid_field(field)) return {SFNTT_INVALID_ARGUMENT, "unknown field"};
   return {};
@@ -175,7 +178,7 @@ Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out
       if (sfntt::is_monty(field))
         SFNTT_TRY(sfntt::monty_lde_dev(ctx, field, din[k], dout[k], log_n, cols, added_bits, shift_monty, mode, comp));
       else
-        SFNTT_TRY(sfntt::m31_lde_dev(ctx, din[k], dout[k], log_n, cols, added_bits, comp));
+        SFNTT_TRY(sfntt::m31_lde_dev(ctx, din[k], dout[k], log_n, cols, added_bits, comp, mode == kCircleLde));
       SFNTT_CU(cudaEventRecord(t1[c], comp));
       SFNTT_CU(cudaEventRecord(slot[k].computed, comp));
       SFNTT_CU(cudaStreamWaitEvent(down, slot[k].computed, 0));
@@ -220,7 +223,8 @@ int api_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, uint32_t 
   if (field == SFNTT_M31 && log_ext > 30) s = {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (s.ok() && len != ((size_t)batch << log_n))  // src/lde/mod.rs:54-56
     s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != batch << log_n"};
-  if (s.ok() && (mode & ~(SFNTT_LDE_UNFUSED | SFNTT_LDE_NATURAL))) s = {SFNTT_INVALID_ARGUMENT, "unknown mode"};
+  if (s.ok() && (field == SFNTT_M31 ? (mode != 0 && mode != kCircleLde) : (mode & ~(SFNTT_LDE_UNFUSED | SFNTT_LDE_NATURAL))))
+    s = {SFNTT_INVALID_ARGUMENT, "unknown mode"};
   if (s.ok() && len && (!in || !out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
   if (s.ok() && len) s = run_host_lde(ctx, field, in, out, log_n, batch, added_bits, shift_monty, mode, ns);
   return finish(ctx, s);
@@ -269,6 +273,8 @@ void sfntt_ctx_destroy(sfntt_ctx* ctx) {
     for (auto& f : ctx->monty_tw)
       for (auto& b : f) b.release();
     for (auto& m : ctx->m31_tw)
+      for (auto& kv : m) kv.second.release();
+    for (auto& m : ctx->m31c_tw)
       for (auto& kv : m) kv.second.release();
     for (auto& kv : ctx->lde_tabs) kv.second.release();
     ctx->buf_in.release();
@@ -380,6 +386,69 @@ int sfntt_coset_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, u
 int sfntt_m31_lde(sfntt_ctx* ctx, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
                   uint32_t added_bits, uint32_t* out, uint64_t* gpu_ns) {
   return api_lde(ctx, SFNTT_M31, in, len, log_n, batch, added_bits, 0, SFNTT_LDE_FUSED, out, gpu_ns);
+}
+
+int sfntt_circle_lde(sfntt_ctx* ctx, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
+                     uint32_t added_bits, uint32_t* out, uint64_t* gpu_ns) {
+  return api_lde(ctx, SFNTT_M31, in, len, log_n, batch, added_bits, 0, kCircleLde, out, gpu_ns);
+}
+
+int sfntt_circle_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                         uint32_t added_bits, void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  Status s;
+  if (batch && (!d_in || !d_out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  if (s.ok()) s = sfntt::m31_lde_dev(ctx, d_in, d_out, log_n, batch, added_bits, (cudaStream_t)stream, true);
+  return finish(ctx, s);
+}
+
+int sfntt_circle_ntt_dev(sfntt_ctx* ctx, int inverse, uint32_t* d_data, uint32_t log_n, uint32_t batch,
+                         void* stream) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  return finish(ctx, sfntt::circle_ntt_dev(ctx, inverse != 0, d_data, log_n, batch, (cudaStream_t)stream));
+}
+
+int sfntt_circle_ntt(sfntt_ctx* ctx, int inverse, const uint32_t* in, size_t len, uint32_t log_n, uint32_t batch,
+                     uint32_t* out, uint64_t* gpu_ns) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  if (gpu_ns) *gpu_ns = 0;
+  Status s = check_log(SFNTT_M31, log_n);
+  if (s.ok() && len != ((size_t)batch << log_n))
+    s = {SFNTT_INVALID_SIZE, "input length " + std::to_string(len) + " != batch << log_n"};
+  if (s.ok() && len && (!in || !out)) s = {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  if (s.ok() && len) {
+    s = [&]() -> Status {
+      const size_t bytes = len * sizeof(uint32_t);
+      SFNTT_TRY(ctx->buf_in.reserve(bytes));
+      uint32_t* d = ctx->buf_in.as<uint32_t>();
+      SFNTT_CU(cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_start, ctx->stream));
+      SFNTT_TRY(sfntt::circle_ntt_dev(ctx, inverse != 0, d, log_n, batch, ctx->stream));
+      SFNTT_CU(cudaEventRecord(ctx->ev_stop, ctx->stream));
+      SFNTT_CU(cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      SFNTT_CU(cudaStreamSynchronize(ctx->stream));
+      SFNTT_TRY(device_flag(ctx));
+      return elapsed_ns(ctx, gpu_ns);
+    }();
+  }
+  return finish(ctx, s);
+}
+
+int sfntt_prepare_circle(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits) {
+  if (!ctx) return SFNTT_INVALID_ARGUMENT;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  DeviceGuard dg(ctx->device);
+  Status s = check_log(SFNTT_M31, log_n + added_bits);
+  const uint2* tw;
+  for (uint32_t k : {log_n, log_n + added_bits})
+    for (int inv = 0; inv < 2 && s.ok() && k > 0; ++inv) s = sfntt::m31_circle_twiddles(ctx, inv, k, ctx->stream, &tw);
+  return finish(ctx, s);
 }
 
 int sfntt_prepare(sfntt_ctx* ctx, int field, uint32_t log_n) {

@@ -101,6 +101,8 @@ struct sfntt_ctx {
   sfntt::DevBuf monty_tw[2][2];
   uint32_t monty_log[2][2] = {{0, 0}, {0, 0}};
   std::map<uint32_t, sfntt::DevBuf> m31_tw[2];
+  // canonic-coset circle FFT twiddles (same layout as m31_tw)
+  std::map<uint32_t, sfntt::DevBuf> m31c_tw[2];
   // LDE multiplier and twist tables keyed by (field, log_n, added_bits, shift, kind)
   std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, int>, sfntt::DevBuf> lde_tabs;
 
@@ -142,6 +144,7 @@ inline int monty_slot(int field) { return field == SFNTT_KOALABEAR ? 1 : 0; }
 Status monty_twiddles(sfntt_ctx* ctx, int field, bool inverse, uint32_t log_n, cudaStream_t stream,
                       const uint2** out);
 Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
+Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
 // kind 0: fused LDE multipliers M_q[i] = n^-1 (shift g^{rev(q)})^i, q < 2^added, i < n
 // kind 1: plain shift powers shift^i, i < n_ext (unfused path)
 Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
@@ -171,8 +174,13 @@ Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in
 // Coset LDE over BabyBear or KoalaBear (lde.cu).
 Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n,
                      uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t stream);
+// canonic = false: the reference-network composition inverse(odds(log_n)) ->
+// zero-pad -> forward(odds(log_n + added)); true: the canonic-coset circle LDE
+// (same network, canonic circle-FFT twiddles).
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
-                   uint32_t added_bits, cudaStream_t stream);
+                   uint32_t added_bits, cudaStream_t stream, bool canonic = false);
+// Canonic-coset circle FFT (evaluate) / inverse (interpolate, times n^-1), in place.
+Status circle_ntt_dev(sfntt_ctx* ctx, bool inverse, uint32_t* d, uint32_t log_n, uint32_t batch, cudaStream_t stream);
 // n^-1 mod p, canonical (ntt.cu).
 uint32_t inv_n_of(int field, uint32_t log_n);
 // Row-order / row-major permutations of SoA batches (layout.cu); bitrev_cols_dev

@@ -35,9 +35,6 @@
 
 namespace sfntt {
 
-Status ntt_layers_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint64_t stride, uint32_t log_n,
-                      uint32_t batch, uint32_t a, uint32_t b, cudaStream_t s);
-
 namespace {
 
 struct ExpandArgs {
@@ -338,26 +335,32 @@ Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* 
 }
 
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
-                   uint32_t added_bits, cudaStream_t s) {
+                   uint32_t added_bits, cudaStream_t s, bool canonic) {
   const uint32_t log_ext = log_n + added_bits;
   if (log_ext > 30) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (batch == 0) return {};
   const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
+  auto twiddles = [&](bool inverse, uint32_t k, const uint2** tw) {
+    return canonic ? m31_circle_twiddles(ctx, inverse, k, s, tw) : m31_twiddles(ctx, inverse, k, s, tw);
+  };
+  const uint2 *tw_inv = nullptr, *tw_fwd = nullptr;
+  if (log_n > 0) {  // log n = 0: the copy and the replication need no twiddles
+    SFNTT_TRY(twiddles(true, log_n, &tw_inv));
+    SFNTT_TRY(twiddles(false, log_ext, &tw_fwd));
+  }
   if (!ctx->no_tma && log_n >= 13 && added_bits <= 4 && aligned16(d_in) && aligned16(d_out)) {
     // I1: inverse layers [0, lo) into the output columns; X: inverse layers
     // [lo, log_n), n^-1, and per output block forward layers [lo, log_n) of
     // the extended network; F3: forward layers [0, lo) of the extended network.
     const uint32_t lo = log_n - 8;
-    const uint2 *tw_inv = nullptr, *tw_fwd = nullptr;
-    SFNTT_TRY(m31_twiddles(ctx, true, log_n, s, &tw_inv));
-    SFNTT_TRY(m31_twiddles(ctx, false, log_ext, s, &tw_fwd));
     SFNTT_TRY(layers_dev(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, 0, lo, 0u, tw_inv, s));
     SFNTT_TRY((launch_tma_expand<M31, 8, false>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, tw_inv, tw_fwd,
                                                 nullptr, s, inv_n_of(SFNTT_M31, log_n))));
     return layers_dev(ctx, SFNTT_M31, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, lo, 0u, tw_fwd, s);
   }
   if (log_n > 0) {
-    SFNTT_TRY(ntt_dev_oop(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, true, s));
+    SFNTT_TRY(layers_dev(ctx, SFNTT_M31, true, d_in, d_out, n, n_ext, log_n, batch, 0, log_n, inv_n_of(SFNTT_M31, log_n),
+                         tw_inv, s));
   } else {
     SFNTT_CU(cudaMemcpy2DAsync(d_out, n_ext * 4, d_in, 4, 4, batch, cudaMemcpyDeviceToDevice, s));
   }
@@ -368,8 +371,20 @@ Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32
     replicate_kernel<<<grid ? grid : 1, 256, 0, s>>>(d_out, log_n, log_ext, total);
     SFNTT_TRY(launch_check(ctx, "m31_replicate", s, total * 4u * (1u + (1u << added_bits) - 1u)));
   }
-  if (log_n > 0) SFNTT_TRY(ntt_layers_dev(ctx, SFNTT_M31, false, d_out, n_ext, log_ext, batch, 0, log_n, s));
+  if (log_n > 0)
+    SFNTT_TRY(layers_dev(ctx, SFNTT_M31, false, d_out, d_out, n_ext, n_ext, log_ext, batch, 0, log_n, 0u, tw_fwd, s));
   return {};
+}
+
+Status circle_ntt_dev(sfntt_ctx* ctx, bool inverse, uint32_t* d, uint32_t log_n, uint32_t batch, cudaStream_t s) {
+  if (log_n > 30) return {SFNTT_INVALID_SIZE, "M31 log_n > 30"};
+  if (log_n == 0 || batch == 0) return {};
+  if (!d) return {SFNTT_INVALID_ARGUMENT, "null buffer"};
+  const uint2* tw = nullptr;
+  SFNTT_TRY(m31_circle_twiddles(ctx, inverse, log_n, s, &tw));
+  const uint64_t n = 1ull << log_n;
+  return layers_dev(ctx, SFNTT_M31, inverse, d, d, n, n, log_n, batch, 0, log_n,
+                    inverse ? inv_n_of(SFNTT_M31, log_n) : 0u, tw, s);
 }
 
 }  // namespace sfntt

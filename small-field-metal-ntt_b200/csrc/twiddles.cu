@@ -72,6 +72,32 @@ __global__ void m31_twiddle_kernel(uint2* tab, uint32_t log_n, M31Layers L, int 
   tab[t] = make_uint2(w, shoup_of<M31>(w));
 }
 
+// Canonic-coset circle FFT (Stwo-style; not in the reference): layer L,
+// block b holds y (L = 0) or x (L >= 1) of m G_{2^(k+1)} with
+// m = (1 + 4 bitrev_{k-1-L}(b)) 2^max(L-1, 0), i.e. of the half-coset point
+// h_i = (1 + 4i) G_{2^(k+1)} doubled L - 1 times.
+__global__ void circle_twiddle_kernel(uint2* tab, uint32_t log_n, uint32_t gx, uint32_t gy, int inverse) {
+  const uint32_t n = 1u << log_n;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n - 1u) return;
+  const uint32_t top = 31u - __clz(n - 1u - t);
+  const uint32_t layer = log_n - 1u - top;
+  const uint32_t b = t - (n - (n >> layer));
+  const uint32_t bits = log_n - 1u - layer;
+  const uint32_t i = bits ? (__brev(b) >> (32u - bits)) : 0u;
+  const uint64_t mask = (2ull << log_n) - 1ull;  // m mod 2^(k+1)
+  uint64_t m = ((uint64_t)(1u + 4u * i) << (layer ? layer - 1u : 0u)) & mask;
+  uint32_t rx = 1u, ry = 0u, bx = gx, by = gy;
+  while (m) {
+    if (m & 1u) cadd_dev(rx, ry, bx, by, rx, ry);
+    cadd_dev(bx, by, bx, by, bx, by);
+    m >>= 1;
+  }
+  uint32_t w = layer == 0u ? ry : rx;
+  if (inverse) w = pow_var<M31>(w, M31::P - 2u);
+  tab[t] = make_uint2(w, shoup_of<M31>(w));
+}
+
 struct LdeBases { uint32_t b[16]; };
 
 // kind 0: tab[q*n + i] = n^-1 * base_q^i ; kind 1: tab[i] = base_0^i
@@ -163,6 +189,25 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
     Status s = sync_after_build(ctx, stream, "m31_twiddle_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->m31_tw[d].emplace(log_n, buf).first;
+  }
+  *out = it->second.as<uint2>();
+  return {};
+}
+
+Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out) {
+  const int d = inverse ? 1 : 0;
+  if (log_n == 0 || log_n > 30) return {SFNTT_INVALID_SIZE, "M31 log_n must be in [1, 30]"};
+  auto it = ctx->m31c_tw[d].find(log_n);
+  if (it == ctx->m31c_tw[d].end()) {
+    if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twiddle table not prepared before capture"};
+    DevBuf buf;
+    const uint32_t count = (1u << log_n) - 1u;
+    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    const host::CPoint g = host::subgroup_gen(log_n + 1);
+    circle_twiddle_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_n, g.x, g.y, inverse ? 1 : 0);
+    Status s = sync_after_build(ctx, stream, "circle_twiddle_kernel");
+    if (!s.ok()) { buf.release(); return s; }
+    it = ctx->m31c_tw[d].emplace(log_n, buf).first;
   }
   *out = it->second.as<uint2>();
   return {};

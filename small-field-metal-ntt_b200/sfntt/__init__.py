@@ -441,6 +441,49 @@ class M31Lde:
         _check(self.ctx.handle, st, batch_size << log_n)
 
 
+class CircleLde:
+    """Canonic-coset circle FFT and circle LDE over M31 (Stwo-style): the
+    reference's M31 network and conventions with circle-FFT twiddles (layer 0
+    y(h), layer L >= 1 x(2^(L-1) h)) on odds(log n) ordered half coset then
+    conjugates, values bit-reversed.  The LDE interpolates, zero-pads the
+    coefficients and evaluates on odds(log n + added_bits): a genuine
+    low-degree extension.  No reference counterpart (planned there)."""
+
+    def __init__(self, ctx: Context | None = None, device: int = 0):
+        self.ctx = ctx or default_context(device)
+
+    def ntt(self, data, log_n: int, batch: int = 1, inverse: bool = False):
+        inp = _u32(data)
+        out = np.empty_like(inp)
+        ns = ctypes.c_uint64()
+        st = _ffi.lib().sfntt_circle_ntt(self.ctx.handle, int(inverse), _p(inp), inp.size, log_n, batch, _p(out),
+                                         ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return out, int(ns.value)
+
+    def execute(self, input, log_n: int, batch_size: int, added_bits: int,
+                out: np.ndarray | None = None) -> LdeResult:
+        inp = _u32(input)
+        dst = out if out is not None else np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
+        ns = ctypes.c_uint64()
+        st = _ffi.lib().sfntt_circle_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits, _p(dst),
+                                         ctypes.byref(ns))
+        _check(self.ctx.handle, st, inp.size)
+        return LdeResult(dst, int(ns.value))
+
+    def prepare(self, log_n: int, added_bits: int) -> None:
+        _check(self.ctx.handle, _ffi.lib().sfntt_prepare_circle(self.ctx.handle, log_n, added_bits))
+
+    def execute_dev(self, in_ptr: int, out_ptr: int, log_n: int, batch_size: int, added_bits: int,
+                    stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_circle_lde_dev(self.ctx.handle, in_ptr, out_ptr, log_n, batch_size, added_bits, stream)
+        _check(self.ctx.handle, st, batch_size << log_n)
+
+    def ntt_dev(self, ptr: int, log_n: int, batch: int = 1, inverse: bool = False, stream: int = 0) -> None:
+        st = _ffi.lib().sfntt_circle_ntt_dev(self.ctx.handle, int(inverse), ptr, log_n, batch, stream)
+        _check(self.ctx.handle, st, batch << log_n)
+
+
 class Cm31Ntt:
     """Circle NTT over the M31 quadratic extension CM31 = M31[i]/(i^2+1)
     (planned in the reference, TODOS.md:27-31): `batch` columns of 2^log_n

@@ -41,6 +41,11 @@ SIGNATURES = {
     "sfntt_coset_lde": (i32, [vp, i32, u32p, sz, u32, u32, u32, u32, i32, u32p, u64p]),
     "sfntt_coset_lde_dev": (i32, [vp, i32, vp, vp, u32, u32, u32, u32, i32, vp]),
     "sfntt_to_monty_dev": (i32, [vp, i32, vp, sz, vp]),
+    "sfntt_circle_ntt": (i32, [vp, i32, u32p, sz, u32, u32, u32p, u64p]),
+    "sfntt_circle_lde": (i32, [vp, u32p, sz, u32, u32, u32, u32p, u64p]),
+    "sfntt_prepare_circle": (i32, [vp, u32, u32]),
+    "sfntt_circle_ntt_dev": (i32, [vp, i32, vp, u32, u32, vp]),
+    "sfntt_circle_lde_dev": (i32, [vp, vp, vp, u32, u32, u32, vp]),
     "sfntt_cm31_prepare": (i32, [vp, u32, u32]),
     "sfntt_cm31_ntt_dev": (i32, [vp, i32, vp, u32, u32, vp]),
     "sfntt_cm31_ntt": (i32, [vp, i32, u32p, sz, u32, u32, u32p, u64p]),

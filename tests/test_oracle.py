@@ -365,3 +365,77 @@ def test_cm31_ntt_is_componentwise():
     i_pairs = O.cm31_mul(np.tile(np.array([0, 1], np.uint32), re.size), pairs)
     assert np.array_equal(O.cm31_ntt(i_pairs, log_n, batch),
                           O.cm31_mul(np.tile(np.array([0, 1], np.uint32), re.size), fw))
+
+
+# ---- canonic-coset circle FFT / circle LDE (Stwo-style; not in the reference) ---
+# Pinned here against its definition, evaluated directly in Python integers:
+# domain odds(k) ordered h_0..h_{n/2-1}, conj(h_0).., h_i = (1 + 4i) G_{2^(k+1)};
+# storage r holds f(D[bitrev_k(r)]); coefficient r multiplies
+# y^{r_0} x^{r_1} pi(x)^{r_2} ..., pi(x) = 2x^2 - 1.
+def _cadd(a, b):
+    return ((a[0] * b[0] - a[1] * b[1]) % MP, (a[0] * b[1] + a[1] * b[0]) % MP)
+
+
+def _cmul(p, m):
+    r, b = (1, 0), p
+    while m:
+        if m & 1:
+            r = _cadd(r, b)
+        b = _cadd(b, b)
+        m >>= 1
+    return r
+
+
+def _gen(k):
+    g = (2, 1268011823)  # circle.rs:17-20, order 2^31
+    for _ in range(31 - k):
+        g = _cadd(g, g)
+    return g
+
+
+def _domain(k):
+    n = 1 << k
+    g = _gen(k + 1)
+    half = [_cmul(g, 1 + 4 * i) for i in range(n // 2)]
+    return half + [(x, (-y) % MP) for (x, y) in half]
+
+
+def _basis(r, k, pt):
+    x, y = pt
+    v = y if r & 1 else 1
+    for j in range(1, k):
+        if (r >> j) & 1:
+            v = v * x % MP
+        x = (2 * x * x - 1) % MP
+    return v
+
+
+def _circle_eval(coeffs, k_dom):
+    """Values of sum_r c_r b_r on D_{k_dom}, bit-reversed storage order."""
+    dom = _domain(k_dom)
+    n = 1 << k_dom
+    nat = [sum(int(c) * _basis(r, k_dom, p) for r, c in enumerate(coeffs)) % MP for p in dom]
+    return [nat[_bitrev(r, k_dom)] for r in range(n)]
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 3, 4, 6])
+def test_circle_fft_is_basis_evaluation(log_n):
+    c = O.lcg(1 << log_n, 70 + log_n, MP)
+    assert list(O.circle_ntt(c, log_n)) == _circle_eval(c, log_n)
+    assert np.array_equal(O.circle_ntt(O.circle_ntt(c, log_n), log_n, inverse=True), c)
+
+
+@pytest.mark.parametrize("log_n,added", [(1, 1), (2, 1), (3, 2), (4, 1), (5, 3)])
+def test_circle_lde_is_low_degree_extension(log_n, added):
+    """The extension evaluates, on the bigger canonic coset, the same circle
+    polynomial that interpolates the input: a genuine low-degree extension."""
+    x = O.lcg(2 << log_n, 90 + log_n, MP)
+    out = O.circle_lde(x, log_n, 2, added)
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    for c in range(2):
+        coeffs = O.circle_ntt(x[c * n:(c + 1) * n], log_n, inverse=True)
+        assert list(out[c * n_ext:(c + 1) * n_ext]) == _circle_eval(coeffs, log_n + added)
+    assert np.array_equal(O.circle_lde(x, log_n, 2, added, threads=2), out)
+    tw = O.circle_twiddles(log_n + added)
+    assert np.array_equal(O.circle_twiddles(log_n + added, inverse=True),
+                          np.array([pow(int(t), MP - 2, MP) for t in tw], np.uint32))
