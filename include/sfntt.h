@@ -220,8 +220,8 @@ int sfntt_cm31_ntt(sfntt_ctx *ctx, int inverse, const uint32_t *in, size_t len, 
 int sfntt_cm31_mul_dev(sfntt_ctx *ctx, const uint32_t *d_a, const uint32_t *d_b, uint32_t *d_out, size_t n,
                        void *stream);
 
-/* ---- Uneven batches in one graph launch (no reference counterpart: the
- * north-star batching pattern).  An item is `batch` SoA columns of 2^log_n
+/* ---- Uneven batches in one graph launch (no reference counterpart: many
+ * polynomials of uneven sizes per launch).  An item is `batch` SoA columns of 2^log_n
  * points of any field, extended by 2^added_bits: BabyBear items are the
  * coset LDE of CosetLdeBatch::execute (src/lde/mod.rs:43-107, shift_monty 0 =
  * reference shift), KoalaBear items the same LDE over KoalaBear, M31 items the
