@@ -443,7 +443,18 @@ struct TPass {
         tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
         tma_load(min, geo(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
       }
+      // A wait that ran out is agreed on at the barrier before the store:
+      // the rounds in between touch only in-bounds shared memory and
+      // twiddles whatever the tile holds, and every thread takes the same
+      // barriers, so no extra CTA-wide barrier is needed per tile.
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      const Geo g = geo(a, t);
+      ld<kFirst>(cur, v, tid);
+      if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
+      rounds<0>(cur, v, a, tws, g, tid);
+      finish(v, a, g, tid);
+      st<kLast>(cur, v, tid);
+      tma::fence_proxy_async();
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(a.err, 1);
@@ -452,14 +463,6 @@ struct TPass {
         }
         return;
       }
-      const Geo g = geo(a, t);
-      ld<kFirst>(cur, v, tid);
-      if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
-      rounds<0>(cur, v, a, tws, g, tid);
-      finish(v, a, g, tid);
-      st<kLast>(cur, v, tid);
-      tma::fence_proxy_async();
-      __syncthreads();
       if (tid == 0) {
         tma_store(mout, g, cur);
         tma::commit();
@@ -571,23 +574,20 @@ struct TExpand {
       }
       if constexpr (LSTAGE) {
         // Every thread passed the previous tile's last barrier after its last
-        // twiddle read; the barrier below publishes the new copy.
+        // twiddle read; the barrier here publishes the new copy (the chunk,
+        // a function of t, is the same for the whole CTA).
         const uint32_t chunk = (t / ai.batch) & ((1u << (ai.lo - 5)) - 1u);
         if (chunk != staged) {
           Inv::stage_lchunk(tws_inv, ai.tw, ai.lo, chunk, tid);
           Fwd::stage_lchunk(tws_fwd, ai.tw_fwd, ai.lo, chunk, tid);
           staged = chunk;
+          __syncthreads();
         }
       }
+      // A wait that ran out is agreed on at the barrier before the first
+      // store (the inverse and the first block touch only in-bounds shared
+      // memory, twiddles and multipliers whatever the tile holds).
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicExch(ai.err, 1);
-          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
-          tma::wait_all();
-        }
-        return;
-      }
       const typename Inv::Geo g = Inv::geo(ai, t);
       // position of slot m: pos_base + u + (e << lo)
       const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
@@ -627,7 +627,18 @@ struct TExpand {
         }
         Fwd::template st<0>(ob, v, tid);
         tma::fence_proxy_async();
-        __syncthreads();
+        if (q == 0) {
+          if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+              atomicExch(ai.err, 1);
+              if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+              tma::wait_all();
+            }
+            return;
+          }
+        } else {
+          __syncthreads();
+        }
         if (tid == 0) {
           tma::store_5d(mout, 0, g.s1, 0, (int32_t)q, g.s4, ob);
           tma::commit();
