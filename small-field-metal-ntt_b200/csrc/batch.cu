@@ -67,6 +67,7 @@ std::string key_of(const sfntt_lde_item& it) {
 
 Status check_item(const sfntt_lde_item& it) {
   if (!valid_field(it.field)) return {SFNTT_INVALID_ARGUMENT, "item: unknown field"};
+  if (!ext_fits(it.log_n, it.added_bits, 30)) return {SFNTT_INVALID_SIZE, "item: log_n + added_bits too large"};
   if (it.batch && (!it.d_in || !it.d_out)) return {SFNTT_INVALID_ARGUMENT, "item: null buffer"};
   return {};
 }

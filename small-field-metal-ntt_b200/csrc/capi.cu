@@ -217,6 +217,7 @@ int api_lde(sfntt_ctx* ctx, int field, const uint32_t* in, size_t len, uint32_t 
   Status s;
   const uint32_t log_ext = log_n + added_bits;
   s = check_field(field);
+  if (s.ok() && !sfntt::ext_fits(log_n, added_bits, 30)) s = {SFNTT_INVALID_SIZE, "log_n + added_bits too large"};
   if (s.ok() && sfntt::is_monty(field) && log_ext + 1 > sfntt::host::monty_field(field).two_adicity)
     s = {SFNTT_INVALID_SIZE,
          "log_n + added_bits must be <= " + std::to_string(sfntt::host::monty_field(field).two_adicity - 1)};
@@ -444,7 +445,8 @@ int sfntt_prepare_circle(sfntt_ctx* ctx, uint32_t log_n, uint32_t added_bits) {
   if (!ctx) return SFNTT_INVALID_ARGUMENT;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
-  Status s = check_log(SFNTT_M31, log_n + added_bits);
+  Status s = sfntt::ext_fits(log_n, added_bits, 30) ? check_log(SFNTT_M31, log_n + added_bits)
+                                                    : Status{SFNTT_INVALID_SIZE, "log_n + added_bits too large"};
   const uint2* tw;
   for (uint32_t k : {log_n, log_n + added_bits})
     for (int inv = 0; inv < 2 && s.ok() && k > 0; ++inv) s = sfntt::m31_circle_twiddles(ctx, inv, k, ctx->stream, &tw);
@@ -471,6 +473,7 @@ int sfntt_prepare_lde(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   DeviceGuard dg(ctx->device);
   Status s = check_field(field);
+  if (s.ok() && !sfntt::ext_fits(log_n, added_bits, 30)) s = {SFNTT_INVALID_SIZE, "log_n + added_bits too large"};
   if (s.ok()) s = check_log(field, log_n + added_bits + (sfntt::is_monty(field) ? 1 : 0));
   if (s.ok()) {
     const uint2* tw;

@@ -137,6 +137,10 @@ namespace sfntt {
 inline bool is_monty(int field) { return field == SFNTT_BABYBEAR || field == SFNTT_KOALABEAR; }
 inline bool valid_field(int field) { return field == SFNTT_M31 || is_monty(field); }
 inline int monty_slot(int field) { return field == SFNTT_KOALABEAR ? 1 : 0; }
+// log_n + added_bits <= max_log, without the 32-bit sum wrapping for huge inputs.
+inline bool ext_fits(uint32_t log_n, uint32_t added_bits, uint32_t max_log) {
+  return log_n <= max_log && added_bits <= max_log && log_n + added_bits <= max_log;
+}
 
 // Table accessors (twiddles.cu).  All generate on a miss (allocating) and
 // refuse to do so while `stream` is capturing.  `field` is BabyBear or

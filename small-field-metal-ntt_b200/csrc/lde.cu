@@ -216,9 +216,9 @@ Status monty_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, 
                       uint32_t batch, uint32_t added_bits, uint32_t shift_monty, int mode, cudaStream_t s) {
   constexpr int field = F::kId;
   const host::MontyField& mf = host::monty_field(field);
-  const uint32_t log_ext = log_n + added_bits;
-  if (log_ext + 1 > mf.two_adicity)
+  if (!ext_fits(log_n, added_bits, mf.two_adicity - 1))
     return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(mf.two_adicity - 1)};
+  const uint32_t log_ext = log_n + added_bits;
   if (batch == 0) return {};
   const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
   const bool fused = mode == SFNTT_LDE_FUSED && log_n >= 1 && log_n <= 24 && added_bits <= 4;
@@ -323,9 +323,9 @@ Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* 
     if (!(mode & SFNTT_LDE_NATURAL))
       return monty_lde_rows<F>(ctx, d_in, 1ull << log_n, d_out, log_n, batch, added_bits, shift_monty, form, s);
     const host::MontyField& mf = host::monty_field(field);
-    const uint32_t log_ext = log_n + added_bits;
-    if (log_ext + 1 > mf.two_adicity)
+    if (!ext_fits(log_n, added_bits, mf.two_adicity - 1))
       return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(mf.two_adicity - 1)};
+    const uint32_t log_ext = log_n + added_bits;
     if (batch == 0) return {};
     const uint64_t n_ext = 1ull << log_ext;
     SFNTT_TRY(bitrev_cols_dev(ctx, d_in, 1ull << log_n, d_out, n_ext, log_n, batch, s));
@@ -336,8 +336,8 @@ Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* 
 
 Status m31_lde_dev(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
                    uint32_t added_bits, cudaStream_t s, bool canonic) {
+  if (!ext_fits(log_n, added_bits, 30)) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   const uint32_t log_ext = log_n + added_bits;
-  if (log_ext > 30) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= 30"};
   if (batch == 0) return {};
   const uint64_t n = 1ull << log_n, n_ext = 1ull << log_ext;
   auto twiddles = [&](bool inverse, uint32_t k, const uint2** tw) {

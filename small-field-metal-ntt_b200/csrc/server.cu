@@ -265,7 +265,8 @@ int submit(sfntt_server* sv, const sfntt_lde_item* req, const uint32_t* h_in, ui
   if (h_in) r.item.d_in = nullptr;
   r.item.d_out = nullptr;
   if (r.item.batch && !h_in && !r.item.d_in) return SFNTT_INVALID_ARGUMENT;
-  if (r.item.log_n + r.item.added_bits > 30) return finish(sv->ctx, {SFNTT_INVALID_SIZE, "log_n + added_bits > 30"});
+  if (!sfntt::ext_fits(r.item.log_n, r.item.added_bits, 30))
+    return finish(sv->ctx, {SFNTT_INVALID_SIZE, "log_n + added_bits > 30"});
   const double tiles = (double)((uint64_t)r.item.batch << (r.item.log_n + r.item.added_bits)) / 8192.0;
   r.width = std::min(1.0, tiles / (2.0 * sv->ctx->sm_count));
   if (arena_bytes(r) > sv->budget)

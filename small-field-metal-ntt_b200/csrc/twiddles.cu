@@ -216,9 +216,9 @@ Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStr
 Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
                        int kind, cudaStream_t stream, const uint2** out) {
   const host::MontyField& f = host::monty_field(field);
-  const uint32_t log_ext = log_n + added_bits;
-  if (log_ext + 1 > f.two_adicity)
+  if (!ext_fits(log_n, added_bits, f.two_adicity - 1))
     return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(f.two_adicity - 1)};
+  const uint32_t log_ext = log_n + added_bits;
   if (kind == 0 && added_bits > 4) return {SFNTT_INVALID_ARGUMENT, "fused LDE supports added_bits <= 4"};
   const auto key = std::make_tuple(monty_slot(field), log_n, added_bits, shift_monty, kind);
   auto it = ctx->lde_tabs.find(key);

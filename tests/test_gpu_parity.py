@@ -302,3 +302,22 @@ def test_m31_lde_full_size_sampled_columns(ctx):
     ext = ext.reshape(batch, n_ext)
     assert not ext[:, n:].any()
     assert np.array_equal(ext[:, :n], base.reshape(batch, n))
+
+
+def test_extension_size_cannot_wrap(ctx):
+    """log_n + added_bits is range-checked before it is summed in 32 bits:
+    an added_bits near 2^32 must not wrap into a small, accepted size."""
+    huge = (1 << 32) - 4
+    x = O.lcg(1 << 5, 1, O.BB_P, monty=True)
+    for lde in (sfntt.CosetLdeBatch(ctx), sfntt.KbCosetLdeBatch(ctx), sfntt.M31Lde(ctx), sfntt.CircleLde(ctx)):
+        with pytest.raises(sfntt.InvalidSize):
+            lde.execute(x, 5, 1, huge)
+    with pytest.raises(sfntt.InvalidSize):
+        sfntt.CircleLde(ctx).prepare(5, huge)
+    with pytest.raises(sfntt.InvalidSize):
+        ctx.prepare_lde(BB, 5, huge)
+    import torch
+    d = torch.zeros(64, dtype=torch.int32, device="cuda")
+    items = [{"field": BB, "log_n": 5, "batch": 1, "added_bits": huge, "d_in": d.data_ptr(), "d_out": d.data_ptr()}]
+    with pytest.raises(sfntt.InvalidSize):
+        sfntt.LdeBatch(ctx, items).prepare()
