@@ -11,8 +11,8 @@
 // once.  The reference's own permutation kernel is `bitrev_permute`
 // (shaders/m31/m31_ntt_ct_dit_r2.metal:22-41), one word per thread.
 //
-// Kernels move 32 x 32-word tiles through padded shared memory so that global
-// reads and writes are 128-byte segments:
+// Kernels move tiles through shared memory so that global reads and writes are
+// whole 128- to 512-byte segments:
 //   bitrev_cols: tile (column, mid) holds words (hi << (L-5)) | (mid << 5) | lo
 //     for hi, lo < 32; word (hi, mid, lo) goes to (rev5(lo), rev(mid), rev5(hi));
 //     tiles mid and rev(mid) swap, so the permutation also runs in place.
@@ -61,6 +61,88 @@ __global__ void __launch_bounds__(kLayoutThreads) bitrev_cols_kernel(const uint3
       const uint32_t hi = rev_bits(lane, 5), lo = rev_bits(a, 5);
       da[((uint64_t)a << hi_shift) + lane] = ta[hi][lo];
       if (rmid != mid) db[((uint64_t)a << hi_shift) + lane] = tb[hi][lo];
+    }
+    __syncthreads();
+  }
+}
+
+// The same permutation on 64 x 64-word tiles (log_n >= 12): 256-byte global
+// rows and 32 KB per CTA in flight.  The shared tile is XOR-swizzled, word
+// (r, c) at r * 64 + (c ^ ((r >> 1) & 31)), so a row (fixed r) and the
+// bit-reversed column read (rows rev6(j) for the 32 lanes j, whose r >> 1 are
+// the 32 values rev5(j mod 32)) both touch 32 distinct banks.
+constexpr int kWideThreads = 512;
+
+__device__ __forceinline__ uint32_t swz64(uint32_t r, uint32_t c) { return r * 64u + (c ^ ((r >> 1) & 31u)); }
+
+__global__ void __launch_bounds__(kWideThreads) bitrev_cols64_kernel(const uint32_t* in, uint64_t in_stride,
+                                                                     uint32_t* out, uint64_t out_stride,
+                                                                     uint32_t log_n, uint64_t tiles) {
+  __shared__ uint32_t ta[64 * 64], tb[64 * 64];
+  const uint32_t mbits = log_n - 12;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t hi_shift = log_n - 6;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint64_t col = t >> mbits;
+    const uint32_t mid = (uint32_t)(t & ((1ull << mbits) - 1ull));
+    const uint32_t rmid = rev_bits(mid, mbits);
+    if (mid > rmid) continue;  // uniform over the CTA
+    const uint32_t* sa = in + col * in_stride + ((uint64_t)mid << 6);
+    const uint32_t* sb = in + col * in_stride + ((uint64_t)rmid << 6);
+#pragma unroll
+    for (uint32_t h = warp; h < 64; h += kWideThreads / 32) {
+#pragma unroll
+      for (uint32_t w = lane; w < 64; w += 32) {
+        ta[swz64(h, w)] = sa[((uint64_t)h << hi_shift) + w];
+        if (rmid != mid) tb[swz64(h, w)] = sb[((uint64_t)h << hi_shift) + w];
+      }
+    }
+    __syncthreads();
+    // tile mid's word (hi, lo) lands in tile rmid at row rev6(lo), word rev6(hi), and vice versa
+    uint32_t* da = out + col * out_stride + ((uint64_t)rmid << 6);
+    uint32_t* db = out + col * out_stride + ((uint64_t)mid << 6);
+#pragma unroll
+    for (uint32_t a = warp; a < 64; a += kWideThreads / 32) {
+      const uint32_t lo = rev_bits(a, 6);
+#pragma unroll
+      for (uint32_t j = lane; j < 64; j += 32) {
+        const uint32_t hi = rev_bits(j, 6);
+        da[((uint64_t)a << hi_shift) + j] = ta[swz64(hi, lo)];
+        if (rmid != mid) db[((uint64_t)a << hi_shift) + j] = tb[swz64(hi, lo)];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Row-major on 128-column x 32-row tiles (log_n >= 5, batch >= 128): 128-byte
+// reads (32 rows of one column) and 512-byte writes (128 columns of one row),
+// so a tile's output is 32 runs of 512 bytes, one per output row.  Tile word
+// (column j, row i) at j * 33 + i: a column (fixed j, lanes over i) and a row
+// (fixed i, lanes over j) both touch 32 distinct banks.
+constexpr uint32_t kWideCols = 128;
+
+__global__ void __launch_bounds__(kWideThreads) transpose_wide_kernel(const uint32_t* __restrict__ in,
+                                                                      uint32_t* __restrict__ out, uint32_t log_n,
+                                                                      uint32_t batch, uint32_t cblocks,
+                                                                      uint64_t tiles, int bitrev) {
+  __shared__ uint32_t tile[kWideCols * 33];
+  const uint64_t n = 1ull << log_n;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint32_t cb = (uint32_t)(t % cblocks);
+    const uint64_t r0 = (t / cblocks) << 5;
+    const uint32_t c0 = cb * kWideCols;
+#pragma unroll
+    for (uint32_t j = warp; j < kWideCols; j += kWideThreads / 32)
+      if (c0 + j < batch) tile[j * 33 + lane] = __ldcs(in + (uint64_t)(c0 + j) * n + r0 + lane);
+    __syncthreads();
+#pragma unroll
+    for (uint32_t k = warp; k < 32 * (kWideCols / 32); k += kWideThreads / 32) {
+      const uint32_t i = k / (kWideCols / 32), j = (k % (kWideCols / 32)) * 32 + lane;
+      const uint64_t r = r0 + i;
+      const uint64_t R = bitrev ? rev_bits((uint32_t)r, log_n) : r;
+      if (c0 + j < batch) __stcs(out + R * batch + c0 + j, tile[j * 33 + i]);
     }
     __syncthreads();
   }
@@ -135,6 +217,12 @@ Status bitrev_cols_dev(sfntt_ctx* ctx, const uint32_t* in, uint64_t in_stride, u
     return {};
   }
   launch_begin(ctx, s);
+  if (log_n >= 12) {
+    const uint64_t tiles = (uint64_t)batch << (log_n - 12);
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 4));
+    bitrev_cols64_kernel<<<grid, kWideThreads, 0, s>>>(in, in_stride, out, out_stride, log_n, tiles);
+    return launch_check(ctx, "layout_bitrev_cols", s, total * 8);
+  }
   if (log_n >= 10) {
     const uint64_t tiles = (uint64_t)batch << (log_n - 10);
     bitrev_cols_kernel<<<grid_for(ctx, tiles), kLayoutThreads, 0, s>>>(in, in_stride, out, out_stride, log_n, tiles);
@@ -164,6 +252,13 @@ Status layout_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t lo
     return {};
   }
   launch_begin(ctx, s);
+  if (log_n >= 5 && batch >= kWideCols) {
+    const uint32_t cblocks = (batch + kWideCols - 1) / kWideCols;
+    const uint64_t tiles = (uint64_t)cblocks << (log_n - 5);
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 4));
+    transpose_wide_kernel<<<grid, kWideThreads, 0, s>>>(in, out, log_n, batch, cblocks, tiles, natural ? 1 : 0);
+    return launch_check(ctx, natural ? "layout_transpose_bitrev" : "layout_transpose", s, total * 8);
+  }
   if (log_n >= 5) {
     const uint32_t cblocks = (batch + 31) / 32;
     const uint64_t tiles = (uint64_t)cblocks << (log_n - 5);

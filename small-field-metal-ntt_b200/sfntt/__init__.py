@@ -211,6 +211,12 @@ def default_context(device: int = 0) -> Context:
     return _DEFAULT[device]
 
 
+def _out_words(batch: int, log_n: int, added_bits: int) -> int:
+    """Output length of an extension; 0 when the sizes are out of range, so
+    that the library's own check reports InvalidSize."""
+    return batch << (log_n + added_bits) if log_n + added_bits <= 40 else 0
+
+
 def _u32(a) -> np.ndarray:
     arr = np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
     return arr
@@ -391,8 +397,7 @@ class CosetLdeBatch:
     def execute(self, input, log_n: int, batch_size: int, added_bits: int, shift_monty: int = 0,
                 out: np.ndarray | None = None) -> LdeResult:
         inp = _u32(input)
-        n_out = batch_size << (log_n + added_bits)
-        dst = out if out is not None else np.empty(n_out, dtype=np.uint32)
+        dst = out if out is not None else np.empty(_out_words(batch_size, log_n, added_bits), dtype=np.uint32)
         ns = ctypes.c_uint64()
         st = _ffi.lib().sfntt_coset_lde(self.ctx.handle, self.FIELD, _p(inp), inp.size, log_n, batch_size,
                                         added_bits, shift_monty, self.mode, _p(dst), ctypes.byref(ns))
@@ -428,7 +433,7 @@ class M31Lde:
     def execute(self, input, log_n: int, batch_size: int, added_bits: int,
                 out: np.ndarray | None = None) -> LdeResult:
         inp = _u32(input)
-        dst = out if out is not None else np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
+        dst = out if out is not None else np.empty(_out_words(batch_size, log_n, added_bits), dtype=np.uint32)
         ns = ctypes.c_uint64()
         st = _ffi.lib().sfntt_m31_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits,
                                       _p(dst), ctypes.byref(ns))
@@ -464,7 +469,7 @@ class CircleLde:
     def execute(self, input, log_n: int, batch_size: int, added_bits: int,
                 out: np.ndarray | None = None) -> LdeResult:
         inp = _u32(input)
-        dst = out if out is not None else np.empty(batch_size << (log_n + added_bits), dtype=np.uint32)
+        dst = out if out is not None else np.empty(_out_words(batch_size, log_n, added_bits), dtype=np.uint32)
         ns = ctypes.c_uint64()
         st = _ffi.lib().sfntt_circle_lde(self.ctx.handle, _p(inp), inp.size, log_n, batch_size, added_bits, _p(dst),
                                          ctypes.byref(ns))

@@ -32,7 +32,9 @@ def ctx():
 
 
 @pytest.mark.parametrize("log_n,batch", [(0, 3), (1, 1), (3, 5), (5, 33), (9, 2), (10, 1), (11, 7), (12, 64),
-                                         (14, 3), (16, 1)])
+                                         (14, 3), (16, 1),
+                                         # wide tiles: partial column blocks, one row block, tile pairs
+                                         (6, 100), (13, 65), (15, 130), (17, 3), (5, 128), (9, 300)])
 def test_layout_matches_numpy(ctx, log_n, batch):
     n = 1 << log_n
     x = O.lcg(batch * n, 91 + log_n + batch, O.M31_P)
