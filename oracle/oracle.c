@@ -45,7 +45,7 @@ static const mfield MF_KB = {
     331895189u,   /* 1791270792 * R mod p */
 };
 
-static uint32_t mf_reduce(const mfield *f, uint64_t t) /* babybear.rs:41-51 */
+static inline uint32_t mf_reduce(const mfield *f, uint64_t t) /* babybear.rs:41-51 */
 {
     uint32_t t_lo = (uint32_t)t;
     uint32_t m = t_lo * f->monty_const;
@@ -54,17 +54,17 @@ static uint32_t mf_reduce(const mfield *f, uint64_t t) /* babybear.rs:41-51 */
     return r >= f->p ? r - f->p : r;
 }
 
-static uint32_t mf_to_monty(const mfield *f, uint32_t v) { return mf_reduce(f, (uint64_t)v * f->r2); }
-static uint32_t mf_add(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:113-121 */
+static inline uint32_t mf_to_monty(const mfield *f, uint32_t v) { return mf_reduce(f, (uint64_t)v * f->r2); }
+static inline uint32_t mf_add(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:113-121 */
 {
     uint32_t s = a + b;
     return s >= f->p ? s - f->p : s;
 }
-static uint32_t mf_sub(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:124-130 */
+static inline uint32_t mf_sub(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:124-130 */
 {
     return a >= b ? a - b : f->p - (b - a);
 }
-static uint32_t mf_mul(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:133-137 */
+static inline uint32_t mf_mul(const mfield *f, uint32_t a, uint32_t b) /* babybear.rs:133-137 */
 {
     return mf_reduce(f, (uint64_t)a * b);
 }
@@ -107,29 +107,34 @@ uint32_t orc_kb_two_adic_generator(uint32_t log_n) { return mf_two_adic_generato
 
 #define M31_P ORC_M31_P
 
-uint32_t orc_m31_reduce(uint64_t v) /* m31.rs:54-67 */
+/* The hot helpers are static inline so the NTT loops inline them (the
+ * exported orc_* functions below are thin wrappers): calls to exported
+ * functions of a shared library would otherwise stay out of line. */
+static inline uint32_t m31_reduce_i(uint64_t v) /* m31.rs:54-67 */
 {
     uint32_t lo = (uint32_t)(v & 0x7FFFFFFFu);
     uint32_t hi = (uint32_t)(v >> 31);
     uint32_t s = lo + hi;
     return s >= M31_P ? s - M31_P : s;
 }
-
-uint32_t orc_m31_add(uint32_t a, uint32_t b) { return orc_m31_reduce((uint64_t)a + b); }
-
-uint32_t orc_m31_sub(uint32_t a, uint32_t b) /* m31.rs:38-45 */
+static inline uint32_t m31_add_i(uint32_t a, uint32_t b) { return m31_reduce_i((uint64_t)a + b); } /* m31.rs:32-35 */
+static inline uint32_t m31_sub_i(uint32_t a, uint32_t b) /* m31.rs:38-45 */
 {
     return a >= b ? a - b : M31_P - (b - a);
 }
+static inline uint32_t m31_mul_i(uint32_t a, uint32_t b) { return m31_reduce_i((uint64_t)a * b); } /* m31.rs:48-51 */
 
-uint32_t orc_m31_mul(uint32_t a, uint32_t b) { return orc_m31_reduce((uint64_t)a * b); }
+uint32_t orc_m31_reduce(uint64_t v) { return m31_reduce_i(v); }
+uint32_t orc_m31_add(uint32_t a, uint32_t b) { return m31_add_i(a, b); }
+uint32_t orc_m31_sub(uint32_t a, uint32_t b) { return m31_sub_i(a, b); }
+uint32_t orc_m31_mul(uint32_t a, uint32_t b) { return m31_mul_i(a, b); }
 
 uint32_t orc_m31_inv(uint32_t a) /* m31.rs:69-83 */
 {
     uint32_t result = 1, base = a, e = M31_P - 2;
     while (e > 0) {
-        if (e & 1) result = orc_m31_mul(result, base);
-        base = orc_m31_mul(base, base);
+        if (e & 1) result = m31_mul_i(result, base);
+        base = m31_mul_i(base, base);
         e >>= 1;
     }
     return result;
@@ -351,10 +356,10 @@ static void m31_forward_tw(uint32_t *data, size_t n, uint32_t log_n, const uint3
             uint32_t w = t[block];
             for (size_t j = 0; j < half; j++) {
                 size_t i0 = block * full + j, i1 = i0 + half;
-                uint32_t tmp = orc_m31_mul(data[i1], w); /* butterfly_forward :137-142 */
+                uint32_t tmp = m31_mul_i(data[i1], w); /* butterfly_forward :137-142 */
                 uint32_t v0 = data[i0];
-                data[i0] = orc_m31_add(v0, tmp);
-                data[i1] = orc_m31_sub(v0, tmp);
+                data[i0] = m31_add_i(v0, tmp);
+                data[i1] = m31_sub_i(v0, tmp);
             }
         }
     }
@@ -370,13 +375,13 @@ static void m31_inverse_tw(uint32_t *data, size_t n, uint32_t log_n, const uint3
             for (size_t j = 0; j < half; j++) {
                 size_t i0 = block * full + j, i1 = i0 + half;
                 uint32_t v0 = data[i0], v1 = data[i1]; /* butterfly_inverse :148-153 */
-                data[i0] = orc_m31_add(v0, v1);
-                data[i1] = orc_m31_mul(orc_m31_sub(v0, v1), w);
+                data[i0] = m31_add_i(v0, v1);
+                data[i1] = m31_mul_i(m31_sub_i(v0, v1), w);
             }
         }
     }
-    uint32_t inv_n = orc_m31_inv(orc_m31_reduce(n)); /* cpu_reference.rs:113-117 */
-    for (size_t i = 0; i < n; i++) data[i] = orc_m31_mul(data[i], inv_n);
+    uint32_t inv_n = orc_m31_inv(m31_reduce_i(n)); /* cpu_reference.rs:113-117 */
+    for (size_t i = 0; i < n; i++) data[i] = m31_mul_i(data[i], inv_n);
 }
 
 int orc_m31_forward(uint32_t *data, size_t n)
@@ -609,8 +614,8 @@ void orc_cm31_mul(const uint32_t *a, const uint32_t *b, uint32_t *out, size_t n)
 {
     for (size_t k = 0; k < n; k++) {
         uint32_t ar = a[2 * k], ai = a[2 * k + 1], br = b[2 * k], bi = b[2 * k + 1];
-        uint32_t re = orc_m31_sub(orc_m31_mul(ar, br), orc_m31_mul(ai, bi));
-        uint32_t im = orc_m31_add(orc_m31_mul(ar, bi), orc_m31_mul(ai, br));
+        uint32_t re = m31_sub_i(m31_mul_i(ar, br), m31_mul_i(ai, bi));
+        uint32_t im = m31_add_i(m31_mul_i(ar, bi), m31_mul_i(ai, br));
         out[2 * k] = re;
         out[2 * k + 1] = im;
     }
