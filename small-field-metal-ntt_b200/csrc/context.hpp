@@ -154,6 +154,13 @@ Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStr
 Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
                        int kind, cudaStream_t stream, const uint2** out);
 
+// Tables of the natural-order coset LDE (n >= 2^13): multipliers M_r[p] =
+// n^-1 (shift g_ext^r)^rev(p) (r < 2^added_bits, p < n; within each 2^13-word
+// tile, position 16 t + m is stored at m * 512 + t) and the n-point forward
+// DIT twiddles laid out for columns of 2^added_bits interleaved cosets.
+Status monty_natural_tables(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
+                            cudaStream_t stream, const uint2** mul, const uint2** coset_tw);
+
 // Twist of a strided BabyBear / KoalaBear pass over layers [lo, lo + P),
 // indexed by column position mod 2^(lo+P) (cached like the LDE tables).
 Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream,

@@ -205,9 +205,86 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * (1u + (1u << added_bits)));
 }
 
+// The natural-order expansion (TExpandC): src holds the inverse layers
+// [12, log_n) of every column (stride n); d_out receives the 2x extension with
+// the DIT layers [0, 12) of both interleaved cosets done.
+template <class F>
+Status launch_tma_expand_c(sfntt_ctx* ctx, const uint32_t* src, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                           const uint2* tw_inv, const uint2* tw_fwd, const uint2* mul, cudaStream_t s) {
+  using X = TExpandC<F>;
+  const uint64_t n = 1ull << log_n;
+  CUtensorMap min, mout;
+  SFNTT_TRY(encode_c_map(&min, src, log_n, n, batch));
+  SFNTT_TRY(encode_c_map(&mout, d_out, log_n + 1, 2 * n, batch));
+  TmaArgs a{};
+  a.tw = tw_inv;
+  a.tw_fwd = tw_fwd;
+  a.mul = mul;
+  a.log_n = log_n;
+  a.lo = 0;
+  a.batch = batch;
+  a.log_q = 1;
+  a.err = ctx->err.as<int>();
+  a.spans = 0;
+  a.log_tpc = log_n - kTileBits;
+  a.ntiles = (uint32_t)(((uint64_t)batch * n) >> kTileBits);
+  constexpr int smem = 4 * (int)X::TBYTES + 16 + 16 * (int)X::TW_ENTRIES + 1024;
+  auto kern = tma_expand_c_kernel<F>;
+  static std::atomic<uint64_t> smem_done{0};
+  SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)ctx->sm_count);
+  launch_begin(ctx, s);
+  SFNTT_CU(launch_pdl(kern, grid, X::NT, smem, s, pdl_fits(grid), min, mout, a));
+  static const std::string name = std::string(F::kTag) + "_lde_expand_tma_C12n";
+  return launch_check(ctx, name.c_str(), s, ((uint64_t)batch * n) * 4u * 3u);
+}
+
 }  // namespace
 
 namespace {
+
+// Natural-order 2x LDE without bit-reversal passes (BabyBear / KoalaBear,
+// 2^13 <= n <= 2^20): SI -- the inverse GS-DIF layers [12, log_n) on the
+// natural-order input (strided pass, inverse table) into scratch; XC --
+// TExpandC (inverse layers [0, 12), coset multipliers, forward DIT layers
+// [0, 12) per coset, cosets interleaved); SF -- the forward CT-DIT layers
+// [12, log_n) of every coset on the interleaved extended column (strided pass,
+// coset twiddle table).  *done stays false (nothing launched) when the shape
+// or the state does not allow it: during a capture, it needs its scratch and
+// tables already resident.
+template <class F>
+Status monty_lde_natural2x(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out, uint32_t log_n, uint32_t batch,
+                           uint32_t shift_monty, cudaStream_t s, bool* done) {
+  constexpr int field = F::kId;
+  *done = false;
+  if (ctx->no_tma || log_n < 13 || log_n > 20 || batch == 0 || !aligned16(d_in) || !aligned16(d_out)) return {};
+  const uint64_t n = 1ull << log_n;
+  const size_t bytes = (size_t)(n * batch) * sizeof(uint32_t);
+  if (ctx->buf_aux.bytes < bytes) {
+    if (capturing(s)) return {};  // no allocation during capture: the bit-reversal route needs no scratch
+    SFNTT_TRY(ctx->buf_aux.reserve(bytes));
+  }
+  const uint2 *itw = nullptr, *ftw = nullptr, *mul = nullptr, *ctw = nullptr;
+  Status st = monty_twiddles(ctx, field, true, log_n, s, &itw);
+  if (st.ok()) st = monty_twiddles(ctx, field, false, log_n, s, &ftw);
+  if (st.ok()) st = monty_natural_tables(ctx, field, log_n, 1, shift_monty, s, &mul, &ctw);
+  if (!st.ok()) {
+    if (capturing(s)) return {};  // tables not resident before the capture: the bit-reversal route
+    return st;
+  }
+  uint32_t* mid = ctx->buf_aux.as<uint32_t>();
+  TmaRequest si{};
+  si.in = d_in; si.out = mid; si.in_stride = n; si.out_stride = n; si.tw = itw;
+  si.log_n = log_n; si.lo = 12; si.P = (int)log_n - 12; si.contiguous = false; si.batch = batch;
+  SFNTT_TRY(run_tma_pass_field(ctx, field, true, si, s));
+  SFNTT_TRY(launch_tma_expand_c<F>(ctx, mid, d_out, log_n, batch, itw, ftw, mul, s));
+  TmaRequest sf{};
+  sf.in = d_out; sf.out = d_out; sf.in_stride = 2 * n; sf.out_stride = 2 * n; sf.tw = ctw;
+  sf.log_n = log_n + 1; sf.lo = 13; sf.P = (int)log_n - 12; sf.contiguous = false; sf.batch = batch;
+  SFNTT_TRY(run_tma_pass_field(ctx, field, false, sf, s));
+  *done = true;
+  return {};
+}
 
 // Input columns at stride in_stride (n, or n_ext when they already sit in the
 // output columns); output bit-reversed rows.  F is BabyBear or KoalaBear.
@@ -327,6 +404,11 @@ Status monty_lde_dev(sfntt_ctx* ctx, int field, const uint32_t* d_in, uint32_t* 
       return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(mf.two_adicity - 1)};
     const uint32_t log_ext = log_n + added_bits;
     if (batch == 0) return {};
+    if (form == SFNTT_LDE_FUSED && added_bits == 1) {
+      bool done = false;
+      SFNTT_TRY(monty_lde_natural2x<F>(ctx, d_in, d_out, log_n, batch, shift_monty, s, &done));
+      if (done) return {};
+    }
     const uint64_t n_ext = 1ull << log_ext;
     SFNTT_TRY(bitrev_cols_dev(ctx, d_in, 1ull << log_n, d_out, n_ext, log_n, batch, s));
     SFNTT_TRY(monty_lde_rows<F>(ctx, d_out, n_ext, d_out, log_n, batch, added_bits, shift_monty, form, s));

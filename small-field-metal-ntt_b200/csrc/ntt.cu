@@ -12,12 +12,6 @@
 
 namespace sfntt {
 
-static Status run_tma_pass(sfntt_ctx* ctx, int field, bool desc, const TmaRequest& r, cudaStream_t s) {
-  if (field == SFNTT_BABYBEAR) return desc ? run_tma_pass_bb_fwd(ctx, r, s) : run_tma_pass_bb_inv(ctx, r, s);
-  if (field == SFNTT_KOALABEAR) return desc ? run_tma_pass_kb_fwd(ctx, r, s) : run_tma_pass_kb_inv(ctx, r, s);
-  return desc ? run_tma_pass_m31_fwd(ctx, r, s) : run_tma_pass_m31_inv(ctx, r, s);
-}
-
 // TMA plan for layers [0, b): one contiguous pass of 5..12 layers, then
 // strided passes of 8 layers.
 static int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
@@ -102,7 +96,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
       }
     }
     if (ok) {
-      for (int i = 0; i < kt; ++i) SFNTT_TRY(run_tma_pass(ctx, field, !inverse, req[i], s));
+      for (int i = 0; i < kt; ++i) SFNTT_TRY(run_tma_pass_field(ctx, field, !inverse, req[i], s));
       return {};
     }
   }

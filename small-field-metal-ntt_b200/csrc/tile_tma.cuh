@@ -649,6 +649,137 @@ struct TExpand {
   }
 };
 
+// Natural-order LDE expansion (BabyBear / KoalaBear, 2x), the mirror image of
+// TExpand for natural-order input and output rows.  The strided pass before it
+// ran the inverse GS-DIF layers [12, log n) on the natural-order evaluations;
+// per contiguous 2^13-word tile this kernel runs the inverse layers [0, 12)
+// (GS-DIF, inverse table), which leaves n * coefficient rev(p) at position p,
+// then for each coset r in {0, 1}: multiplies by M_r[p] = n^-1 (shift
+// g_ext^r)^rev(p) and runs the forward CT-DIT layers [0, 12) of the n-point
+// network (forward table).  Coset r's word p belongs at extended position
+// 2p + r, so both cosets are interleaved in shared memory and the tile leaves
+// as 2^14 contiguous words; the strided pass after it runs the DIT layers
+// [12, log n) of every coset on the interleaved column.  The inverse ends and
+// the forward starts in round 0's layout, so the coefficients stay in
+// registers.
+template <class F>
+struct TExpandC {
+  using Inv = TPass<F, true, Kind::C, 12>;
+  using Fwd = TPass<F, false, Kind::C, 12>;
+  static constexpr int K = Inv::K, E = Inv::E, NT = Inv::NT, R = Inv::R, LT = Inv::LT;
+  static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
+  static constexpr uint32_t TW_ENTRIES = Inv::TW_ENTRIES;  // per direction
+  static_assert(F::kMontgomery, "natural-order expansion: BabyBear / KoalaBear");
+  static_assert(Inv::kLast == 0 && Fwd::kFirst == 0, "inverse ends and forward starts in round 0's layout");
+  using ML = RM<Kind::C, 12, LT, R, K - 1>;
+
+  // Multipliers of the thread's slots (round 0 layout: tile word 16 tid + m)
+  // from mq = M_r + pos_base; the table stores word 16 t + m of a tile at
+  // m * NT + t, so each slot's load is coalesced across the CTA.
+  static_assert(NT == 512 && E == 16, "tile word of round-0 slot m is 16 tid + m");
+  __device__ static __forceinline__ void load_mul(uint2 (&w)[E], const uint2* mq, uint32_t tid) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) w[m] = __ldg(mq + (uint32_t)m * NT + tid);
+  }
+
+  // coset r's values (round K-1 layout, canonical) to the interleaved output tile
+  __device__ static __forceinline__ void put(uint32_t* ostage, const uint32_t (&v)[E], uint32_t ctl, uint32_t r) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const uint32_t e = ((ctl | ML::cm(m)) << 1) | r;  // 14-bit extended word of the tile
+      ostage[(e >> 13) * TWORDS + Inv::sw(e & (TWORDS - 1u))] = v[m];
+    }
+  }
+
+  __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
+    extern __shared__ __align__(1024) uint32_t smem_words[];
+    uint32_t* stage = smem_words;           // 2 x TWORDS: input tiles (double-buffered)
+    uint32_t* ostage = stage + 2 * TWORDS;  // 2 x TWORDS: the tile's two output halves
+    uint64_t* bar = reinterpret_cast<uint64_t*>(ostage + 2 * TWORDS);
+    uint2* tws_inv = reinterpret_cast<uint2*>(bar + 2);
+    uint2* tws_fwd = tws_inv + TW_ENTRIES;
+    const uint32_t tid = threadIdx.x;
+    const TmaArgs& a = args;
+    uint32_t t = blockIdx.x;
+    if (t >= a.ntiles) return;
+    Inv::stage_twiddles(tws_inv, a.tw, tid);
+    Fwd::stage_twiddles(tws_fwd, a.tw_fwd, tid);
+    if (tid == 0) {
+      tma::prefetch_map(min);
+      tma::prefetch_map(mout);
+      tma::mbar_init(&bar[0], 1);
+      tma::mbar_init(&bar[1], 1);
+      tma::fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tma::mbar_expect_tx(&bar[0], TBYTES);
+      Inv::tma_load(min, Inv::geo(a, t), stage, &bar[0]);
+    }
+    const uint32_t ctl = ML::ctid(tid);
+    const uint64_t n = 1ull << a.log_n;
+    uint32_t x[E], v[E];
+    for (uint32_t it = 0; t < a.ntiles; t += gridDim.x, ++it) {
+      const uint32_t buf = it & 1u;
+      uint32_t* cur = stage + buf * TWORDS;
+      const uint32_t tn = t + gridDim.x;
+      if (tid == 0) {
+        // The other input buffer was last read by this CTA's previous tile
+        // (all threads are past its barriers); ostage, by the previous tile's
+        // stores: wait for them here, the barrier before this tile's first
+        // ostage write publishes it.
+        tma::wait_reads();
+        if (tn < a.ntiles) {
+          tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
+          Inv::tma_load(min, Inv::geo(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+        }
+      }
+      const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      const typename Inv::Geo g = Inv::geo(a, t);
+      uint2 w[E];
+      load_mul(w, a.mul + g.pos_base, tid);  // coset 0's, in flight during the inverse layers
+      Inv::template ld<Inv::kFirst>(cur, x, tid);
+      Inv::template rounds<0>(cur, x, a, tws_inv, g, tid);  // x: round 0 layout, canonical
+#pragma unroll
+      for (uint32_t r = 0; r < 2; ++r) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
+        if (r == 0) load_mul(w, a.mul + n + g.pos_base, tid);  // coset 1's, during coset 0's layers
+        Fwd::template rounds<0>(cur, v, a, tws_fwd, g, tid);
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = reduce2p<F>(v[m]);  // lazy CT values to [0, p)
+        // coset 0: every thread is done exchanging through cur before coset 1
+        // reuses it, and ostage is free (thread 0 waited at the tile start)
+        if (r == 0) __syncthreads();
+        put(ostage, v, ctl, r);
+      }
+      tma::fence_proxy_async();
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicExch(a.err, 1);
+          if (tn < a.ntiles) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          tma::wait_all();
+        }
+        return;
+      }
+      if (tid == 0) {
+        // extended rows [2 * pos_base, 2 * pos_base + 2^14) of the column, two boxes of 2^13 words
+        tma::store_3d(mout, 0, 2 * g.c1, g.c2, ostage);
+        tma::store_3d(mout, 0, 2 * g.c1 + (int32_t)(TWORDS / 32), g.c2, ostage + TWORDS);
+        tma::commit();
+      }
+    }
+    if (tid == 0) tma::wait_all();
+  }
+};
+
+template <class F>
+__global__ void __launch_bounds__(TExpandC<F>::NT, 1)
+tma_expand_c_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
+  pdl_enter();
+  TExpandC<F>::run(&min, &mout, a);
+}
+
 template <class F, int P, bool PLAIN, bool LSTAGE>
 __global__ void __launch_bounds__(TExpand<F, P, PLAIN, LSTAGE>::NT, 1)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {

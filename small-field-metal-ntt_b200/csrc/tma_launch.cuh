@@ -162,4 +162,10 @@ Status run_tma_pass_kb_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 Status run_tma_pass_m31_fwd(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 Status run_tma_pass_m31_inv(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s);
 
+inline Status run_tma_pass_field(sfntt_ctx* ctx, int field, bool desc, const TmaRequest& r, cudaStream_t s) {
+  if (field == SFNTT_BABYBEAR) return desc ? run_tma_pass_bb_fwd(ctx, r, s) : run_tma_pass_bb_inv(ctx, r, s);
+  if (field == SFNTT_KOALABEAR) return desc ? run_tma_pass_kb_fwd(ctx, r, s) : run_tma_pass_kb_inv(ctx, r, s);
+  return desc ? run_tma_pass_m31_fwd(ctx, r, s) : run_tma_pass_m31_inv(ctx, r, s);
+}
+
 }  // namespace sfntt

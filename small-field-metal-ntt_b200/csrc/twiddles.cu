@@ -131,6 +131,40 @@ __global__ void twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_mon
   tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
+// Natural-order LDE multipliers M_r[i] = n^-1 base_r^rev(i), stored in the
+// order a contiguous 2^13-word tile's 512 threads read them in the first
+// round (thread t's slot m is word 16 t + m of the tile): entry m * 512 + t
+// of each tile, so one slot's load is a coalesced run across the CTA.
+template <class F>
+__global__ void natural_mul_kernel(uint2* tab, uint32_t log_n, uint32_t count, LdeBases bases,
+                                   uint32_t scale_monty) {
+  const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= count) return;
+  const uint32_t r = o >> log_n;
+  const uint32_t local = o & ((1u << log_n) - 1u);
+  const uint32_t w = local & 8191u;
+  const uint32_t i = (local & ~8191u) | ((w & 511u) << 4) | (w >> 9);
+  uint32_t v = pow_var<F>(bases.b[r], __brev(i) >> (32u - log_n));
+  v = to_canonical(F{}, mul_var<F>(v, scale_monty));
+  tab[o] = make_uint2(v, shoup_of<F>(v));
+}
+
+// Forward twiddles of the n-point DIT, laid out as an extended table for
+// columns that interleave 2^b cosets (word p 2^b + r): layer L (offset
+// 2^L - 1) holds tab[L][j] = g_{L+1-b}^(j >> b) for L >= b, so the strided
+// pass's per-position lookup tab[L][pos mod 2^L] of the extended column finds
+// layer L - b's twiddle of coset position pos >> b.
+template <class F>
+__global__ void coset_twiddle_kernel(uint2* tab, uint32_t count, uint32_t b, MontyGens gens) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const uint32_t L = 31u - __clz(t + 1u);
+  const uint32_t j = t + 1u - (1u << L);
+  uint32_t w = 0;
+  if (L >= b) w = to_canonical(F{}, pow_var<F>(gens.g[L - b], j >> b));
+  tab[t] = make_uint2(w, shoup_of<F>(w));
+}
+
 Status sync_after_build(sfntt_ctx* ctx, cudaStream_t stream, const char* what) {
   SFNTT_TRY(launch_check(ctx, what));
   SFNTT_CU(cudaStreamSynchronize(stream));
@@ -210,6 +244,58 @@ Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStr
     it = ctx->m31c_tw[d].emplace(log_n, buf).first;
   }
   *out = it->second.as<uint2>();
+  return {};
+}
+
+Status monty_natural_tables(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
+                            cudaStream_t stream, const uint2** mul, const uint2** coset_tw) {
+  const host::MontyField& f = host::monty_field(field);
+  if (!ext_fits(log_n, added_bits, f.two_adicity - 1) || added_bits > 4 || log_n < 13)
+    return {SFNTT_INVALID_SIZE, "natural-order LDE tables: 2^13 <= n and log_n + added_bits within the field"};
+  const uint32_t log_ext = log_n + added_bits;
+  const auto kmul = std::make_tuple(monty_slot(field), log_n, added_bits, shift_monty, 3);
+  const auto ktw = std::make_tuple(monty_slot(field), log_n, added_bits, 0u, 4);
+  auto im = ctx->lde_tabs.find(kmul);
+  if (im == ctx->lde_tabs.end()) {
+    if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "LDE table not prepared before capture"};
+    // coset r of the natural-order output: M_r[p] = n^-1 (shift g_ext^r)^rev(p)
+    const uint32_t shift = shift_monty ? host::from_monty(f, shift_monty) : host::two_adic_generator(f, log_ext + 1);
+    const uint32_t g_ext = host::two_adic_generator(f, log_ext);
+    LdeBases B{};
+    for (uint32_t r = 0; r < (1u << added_bits); ++r)
+      B.b[r] = host::to_monty(f, host::mulmod(shift, host::powmod(g_ext, r, f.p), f.p));
+    const uint32_t count = 1u << log_ext;
+    const uint32_t scale = host::to_monty(f, host::invmod(1u << log_n, f.p));
+    DevBuf buf;
+    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    with_monty(field, [&](auto fld) {
+      natural_mul_kernel<decltype(fld)><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_n, count, B,
+                                                                                scale);
+      return 0;
+    });
+    Status s = sync_after_build(ctx, stream, "natural_mul_kernel");
+    if (!s.ok()) { buf.release(); return s; }
+    im = ctx->lde_tabs.emplace(kmul, buf).first;
+  }
+  auto it = ctx->lde_tabs.find(ktw);
+  if (it == ctx->lde_tabs.end()) {
+    if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "LDE table not prepared before capture"};
+    MontyGens g{};
+    for (uint32_t l = 0; l < f.two_adicity; ++l) g.g[l] = host::to_monty(f, host::two_adic_generator(f, l + 1));
+    const uint32_t count = (1u << log_ext) - 1u;
+    DevBuf buf;
+    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    with_monty(field, [&](auto fld) {
+      coset_twiddle_kernel<decltype(fld)><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), count,
+                                                                                  added_bits, g);
+      return 0;
+    });
+    Status s = sync_after_build(ctx, stream, "coset_twiddle_kernel");
+    if (!s.ok()) { buf.release(); return s; }
+    it = ctx->lde_tabs.emplace(ktw, buf).first;
+  }
+  *mul = im->second.as<uint2>();
+  *coset_tw = it->second.as<uint2>();
   return {};
 }
 

@@ -77,7 +77,10 @@ def test_layout_rejects_bad_buffers(ctx):
 
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("log_n,batch,added,shift", [(10, 3, 1, 0), (13, 2, 2, 0), (14, 3, 1, 31), (6, 2, 3, 31),
-                                                     (0, 2, 2, 0), (16, 2, 1, 31)])
+                                                     (0, 2, 2, 0), (16, 2, 1, 31),
+                                                     # 2x, 2^13..2^20: the mirrored network without bit reversals
+                                                     (13, 1, 1, 0), (13, 3, 1, 31), (15, 5, 1, 0), (17, 16, 1, 31),
+                                                     (18, 2, 1, 7), (12, 4, 1, 31)])
 def test_natural_lde_is_plonky3_convention(ctx, fused, log_n, batch, added, shift):
     """Natural-order evaluations in, natural-order rows out: the reference LDE
     conjugated by the bit-reversal permutation on both sides."""
@@ -105,3 +108,32 @@ def test_natural_lde_device_path_2_20(ctx):
         col = x_nat.reshape(batch, -1)[c]
         ref = O.bb_coset_lde(_natural(col, log_n, 1), log_n, 1, added, threads=8)
         assert np.array_equal(got[c], _natural(ref, log_n + added, 1)), c
+
+
+def test_natural_lde_in_graph_with_and_without_scratch(ctx):
+    """Captured in a CUDA graph the natural-order 2x LDE either takes the
+    no-bit-reversal route (scratch already reserved by an earlier call) or
+    falls back to the bit-reversal route (fresh context): same results."""
+    import torch
+    log_n, batch, added = 14, 4, 1
+    x_nat = O.lcg(batch << log_n, 77, O.BB_P, monty=True)
+    ref = _natural(O.bb_coset_lde(_natural(x_nat, log_n, batch), log_n, batch, added, threads=4), log_n + added, batch)
+    for warm in (True, False):
+        c = sfntt.Context(0)
+        c.prepare_lde(sfntt.FIELD_BABYBEAR, log_n, added)
+        lde = sfntt.CosetLdeBatch(c, natural=True)
+        d_in = torch.from_numpy(x_nat.view(np.int32).copy()).cuda()
+        d_out = torch.zeros(batch << (log_n + added), dtype=torch.int32, device="cuda")
+        if warm:
+            lde.execute_dev(d_in.data_ptr(), d_out.data_ptr(), log_n, batch, added)
+            torch.cuda.synchronize()
+            d_out.zero_()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            lde.execute_dev(d_in.data_ptr(), d_out.data_ptr(), log_n, batch, added,
+                            stream=torch.cuda.current_stream().cuda_stream)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(d_out.cpu().numpy().view(np.uint32), ref), warm
+        del g
+        c.close()
