@@ -49,6 +49,10 @@ struct TmaArgs {
   // twist[pos & twist_mask]; nullptr = none
   const uint2* twist;
   uint32_t twist_mask;
+  // M31 contiguous passes: the table's copy of layers 0..3 in first-round
+  // order (entry n of an M31 table with n >= 2^13; see round0_permute_kernel);
+  // nullptr = read the layers from the table itself
+  const uint2* tw0;
   // fused LDE expansion (Expand kernel only)
   const uint2* tw_fwd;
   const uint2* mul;
@@ -140,6 +144,16 @@ struct TPass {
   // layer-beta twiddle tw[beta][e mod 2^beta] is the same for every lane (the
   // per-position remainder is the boundary twist).
   static constexpr bool kStaged = F::kMontgomery && (KD == Kind::C || PLAIN);
+
+  // M31 contiguous passes whose first round gives thread t the tile words
+  // 16 t .. 16 t + 15 (four layers, thread bits 4..12 in order) read that
+  // round's per-block twiddles from the table's first-round copy (TmaArgs::tw0).
+  static constexpr bool round0_linear() {
+    const RoundMap mp = make_map<KD, P, (KD == Kind::C) ? (kTileBits - P) : 5, 4>(0);
+    return Plan<P, 4>::r(0) == 4 && mp.mpos[0] == 0 && mp.mpos[1] == 1 && mp.mpos[2] == 2 && mp.mpos[3] == 3 &&
+           mp.ngrp == 1 && mp.gshift[0] == 4 && mp.gmask[0] == (1u << (kTileBits - 4)) - 1u;
+  }
+  static constexpr bool kRound0Copy = !F::kMontgomery && KD == Kind::C && round0_linear();
   static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
 
   // ---- twiddles: per-layer base pointer + compile-time offset per slot ----
@@ -192,18 +206,39 @@ struct TPass {
         const uint32_t beta = (uint32_t)(b + j);
         const uint32_t L = a.lo + beta;
         const uint32_t n = 1u << a.log_n;
-        const uint2* base = a.tw + (n - (n >> L));
-        if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1));
-        else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
         uint2 tv[E / 2];
-        if (j == r - 1) {
-          tv[0] = __ldg(base);
-        } else {
+        bool copied = false;
+        if constexpr (kRound0Copy && k == 0) {
+          if (a.tw0) {
+            // the table's first-round copy: [tile][layer][pair][thread], coalesced across the CTA
+            const uint2* t0 = a.tw0 + (g.pos_base >> 13) * 7680u;
+            const uint32_t off = j == 0 ? 0u : j == 1 ? 4096u : j == 2 ? 6144u : 7168u;
+            if (j == r - 1) {
+              tv[0] = __ldg(t0 + off + tid);
+            } else {
 #pragma unroll
-          for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
-            const uint4 q = __ldg(reinterpret_cast<const uint4*>(base + o));
-            tv[o] = make_uint2(q.x, q.y);
-            tv[o + 1] = make_uint2(q.z, q.w);
+              for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(t0 + off) + (uint32_t)(o >> 1) * NT + tid);
+                tv[o] = make_uint2(q.x, q.y);
+                tv[o + 1] = make_uint2(q.z, q.w);
+              }
+            }
+            copied = true;
+          }
+        }
+        if (!copied) {
+          const uint2* base = a.tw + (n - (n >> L));
+          if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1));
+          else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
+          if (j == r - 1) {
+            tv[0] = __ldg(base);
+          } else {
+#pragma unroll
+            for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
+              const uint4 q = __ldg(reinterpret_cast<const uint4*>(base + o));
+              tv[o] = make_uint2(q.x, q.y);
+              tv[o + 1] = make_uint2(q.z, q.w);
+            }
           }
         }
 #pragma unroll

@@ -100,6 +100,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch));
     a.spans = n < kTileWords;
     a.log_tpc = a.spans ? 0u : r.log_n - kTileBits;
+    // every M31 table with n >= 2^13 carries its first-round copy from entry n on
+    if constexpr (T::kRound0Copy) a.tw0 = a.spans ? nullptr : r.tw + n;
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> kTileBits);
   } else {
     const uint64_t hb = n >> (r.lo + P);

@@ -98,6 +98,30 @@ __global__ void circle_twiddle_kernel(uint2* tab, uint32_t log_n, uint32_t gx, u
   tab[t] = make_uint2(w, shoup_of<M31>(w));
 }
 
+// M31 tables with n >= 2^13 carry, from entry n on, a copy of layers 0..3
+// in the order the first round of a contiguous 2^13-word tile reads them:
+// thread t owns tile words 16 t .. 16 t + 15, so its layer-L twiddles are the
+// 2^(3-L) consecutive entries from ((tile base + 16 t) >> (L+1)).  Per tile,
+// 7680 pairs: layer 0 as [pair k < 4][t] 128-bit words, layer 1 [k < 2][t],
+// layer 2 [t], layer 3 [t] single pairs, so each load of the round is one
+// contiguous run across the CTA.
+constexpr uint32_t kRound0Pairs = 7680;
+
+__global__ void round0_permute_kernel(uint2* tab, uint32_t log_n) {
+  const uint32_t n = 1u << log_n;
+  const uint32_t total = (n >> 13) * kRound0Pairs;
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const uint32_t T = idx / kRound0Pairs, w = idx - T * kRound0Pairs;
+  uint32_t L, t, o;
+  if (w < 4096) { L = 0; t = (w & 1023u) >> 1; o = 2 * (w >> 10) + (w & 1u); }
+  else if (w < 6144) { L = 1; t = ((w - 4096) & 1023u) >> 1; o = 2 * ((w - 4096) >> 10) + (w & 1u); }
+  else if (w < 7168) { L = 2; t = (w - 6144) >> 1; o = w & 1u; }
+  else { L = 3; t = w - 7168; o = 0; }
+  const uint32_t src = (n - (n >> L)) + ((T * 8192u + 16u * t) >> (L + 1)) + o;
+  tab[n + idx] = tab[src];
+}
+
 struct LdeBases { uint32_t b[16]; };
 
 // kind 0: tab[q*n + i] = n^-1 * base_q^i ; kind 1: tab[i] = base_0^i
@@ -165,6 +189,17 @@ __global__ void coset_twiddle_kernel(uint2* tab, uint32_t count, uint32_t b, Mon
   tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
+size_t m31_table_bytes(uint32_t log_n) {
+  const size_t n = (size_t)1 << log_n;
+  return (log_n >= 13 ? n + (n >> 13) * kRound0Pairs : n - 1) * sizeof(uint2);
+}
+
+void add_round0_copy(uint2* tab, uint32_t log_n, cudaStream_t stream) {
+  if (log_n < 13) return;
+  const uint32_t total = ((1u << log_n) >> 13) * kRound0Pairs;
+  round0_permute_kernel<<<(total + 255) / 256, 256, 0, stream>>>(tab, log_n);
+}
+
 Status sync_after_build(sfntt_ctx* ctx, cudaStream_t stream, const char* what) {
   SFNTT_TRY(launch_check(ctx, what));
   SFNTT_CU(cudaStreamSynchronize(stream));
@@ -211,7 +246,7 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twiddle table not prepared before capture"};
     DevBuf buf;
     const uint32_t count = (1u << log_n) - 1u;
-    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    SFNTT_TRY(buf.reserve(m31_table_bytes(log_n)));
     M31Layers L{};
     // layer l: odds(log_n) doubled l times -> initial = G_{log_n+1-l}, step = G_{log_n-l}
     for (uint32_t l = 0; l < log_n; ++l) {
@@ -220,6 +255,7 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
       L.ix[l] = ini.x; L.iy[l] = ini.y; L.sx[l] = st.x; L.sy[l] = st.y;
     }
     m31_twiddle_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_n, L, inverse ? 1 : 0);
+    add_round0_copy(buf.as<uint2>(), log_n, stream);
     Status s = sync_after_build(ctx, stream, "m31_twiddle_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->m31_tw[d].emplace(log_n, buf).first;
@@ -236,9 +272,10 @@ Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStr
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twiddle table not prepared before capture"};
     DevBuf buf;
     const uint32_t count = (1u << log_n) - 1u;
-    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    SFNTT_TRY(buf.reserve(m31_table_bytes(log_n)));
     const host::CPoint g = host::subgroup_gen(log_n + 1);
     circle_twiddle_kernel<<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_n, g.x, g.y, inverse ? 1 : 0);
+    add_round0_copy(buf.as<uint2>(), log_n, stream);
     Status s = sync_after_build(ctx, stream, "circle_twiddle_kernel");
     if (!s.ok()) { buf.release(); return s; }
     it = ctx->m31c_tw[d].emplace(log_n, buf).first;
