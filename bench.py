@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--added-bits", type=int, default=1)
     ap.add_argument("--mode", default="fused", choices=["fused", "unfused"])
+    ap.add_argument("--natural", action="store_true",
+                    help="BabyBear / KoalaBear LDE in the natural-order convention (Plonky3's coset_lde_batch rows)")
     ap.add_argument("--field", default="bb", choices=["bb", "m31", "kb"],
                     help="bb: the BabyBear coset LDE (the headline); m31: the M31 blow-up of the same shape; "
                          "kb: the KoalaBear coset LDE of the same shape")
@@ -84,6 +86,8 @@ def metric_name(a) -> str:
         return f"M31 blow-up 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
     if a.field == "kb":
         return f"KoalaBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
+    if getattr(a, "natural", False):
+        return f"BabyBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x natural-order rows"
     return METRIC if (a.log_n, a.batch, a.added_bits) == (20, 256, 1) else \
         f"BabyBear coset LDE 2^{a.log_n}x{a.batch} {1 << a.added_bits}x"
 
@@ -100,7 +104,9 @@ def workload(a) -> dict:
             "log_n": a.log_n, "columns": a.batch, "added_bits": a.added_bits, "mode": a.mode,
             "shift": f"g = {g}, row i times {g}^i" if a.shift == "31" else
                      "two_adic_generator(log_n_ext+1) (reference default)",
-            "layout": "SoA column-major, Montgomery u32",
+            "layout": "SoA column-major, Montgomery u32" +
+                      (", natural-order input and output rows" if getattr(a, "natural", False) else
+                       ", bit-reversed input and output rows (the reference's convention)"),
             "l2": f"inputs larger than L2 ({4 * a.batch << a.log_n >> 20} MiB in, "
                   f"{4 * a.batch << (a.log_n + a.added_bits) >> 20} MiB out per step)"}
 
@@ -222,7 +228,9 @@ def cpu_lde_sample(a, target_s: float) -> dict:
     ts = time.perf_counter() - t
     return {"value": ts * 1e3 * a.batch / cols, "unit": "ms", "cores": threads, "kind": "port",
             "sample": f"{cols} of {a.batch} columns (oracle/oracle.c LDE, OpenMP over columns), "
-                      f"scaled x{a.batch / cols:.2f}; 1-thread column time {t1 * 1e3:.1f} ms",
+                      f"scaled x{a.batch / cols:.2f}; 1-thread column time {t1 * 1e3:.1f} ms" +
+                      ("; the reference-order LDE (natural rows add two permutations)" if getattr(a, "natural", False)
+                       else ""),
             "single_thread_ms_full": t1 * 1e3 * a.batch}
 
 
@@ -301,7 +309,8 @@ def main() -> None:
             lde.execute(hin, a.log_n, a.batch, a.added_bits, out=hout)
     else:
         fid = sfntt.FIELD_KOALABEAR if a.field == "kb" else sfntt.FIELD_BABYBEAR
-        lde = (sfntt.KbCosetLdeBatch if a.field == "kb" else sfntt.CosetLdeBatch)(ctx, fused=(a.mode == "fused"))
+        lde = (sfntt.KbCosetLdeBatch if a.field == "kb" else sfntt.CosetLdeBatch)(ctx, fused=(a.mode == "fused"),
+                                                                               natural=a.natural)
         sfntt.convert_monty_dev(ctx, fid, x.data_ptr(), x.numel(), to_monty=True, stream=stream)
         ctx.prepare_lde(fid, a.log_n, a.added_bits, shift)
 
