@@ -330,6 +330,58 @@ class M31Lde {
   Context ctx_;
 };
 
+// Canonic-coset circle FFT and circle LDE over M31 (no reference counterpart):
+// the M31 network with circle-FFT twiddles on odds(log n) ordered half coset
+// then conjugates, values bit-reversed; the LDE interpolates, zero-pads the
+// coefficients and evaluates on odds(log n + added_bits).
+class CircleLde {
+ public:
+  explicit CircleLde(Context ctx = Context()) : ctx_(std::move(ctx)) {}
+  // inverse = false evaluates coefficients, true interpolates (times n^-1); returns (out, device ns)
+  std::pair<std::vector<uint32_t>, uint64_t> ntt(std::span<const uint32_t> in, uint32_t log_n, uint32_t batch,
+                                                 bool inverse) const {
+    std::vector<uint32_t> out(in.size());
+    uint64_t ns = 0;
+    detail::check(ctx_.handle(),
+                  sfntt_circle_ntt(ctx_.handle(), inverse ? 1 : 0, in.data(), in.size(), log_n, batch, out.data(), &ns),
+                  in.size());
+    return {std::move(out), ns};
+  }
+  LdeResult execute(std::span<const uint32_t> input, size_t log_n, size_t batch_size, size_t added_bits) const {
+    LdeResult r;
+    r.data.resize(log_n + added_bits <= 40 ? batch_size << (log_n + added_bits) : 0);
+    detail::check(ctx_.handle(),
+                  sfntt_circle_lde(ctx_.handle(), input.data(), input.size(), (uint32_t)log_n, (uint32_t)batch_size,
+                                   (uint32_t)added_bits, r.data.data(), &r.total_ns),
+                  input.size());
+    return r;
+  }
+
+ private:
+  Context ctx_;
+};
+
+// Circle NTT over CM31 = M31[i]/(i^2+1) columns of interleaved (re, im) pairs
+// (the M31 transform of each coordinate; no reference counterpart).
+class Cm31Ntt {
+ public:
+  explicit Cm31Ntt(Context ctx = Context()) : ctx_(std::move(ctx)) {}
+  // len(pairs) = 2 * (batch << log_n) words; returns (out, device ns)
+  std::pair<std::vector<uint32_t>, uint64_t> ntt(std::span<const uint32_t> pairs, uint32_t log_n, uint32_t batch,
+                                                 bool inverse) const {
+    std::vector<uint32_t> out(pairs.size());
+    uint64_t ns = 0;
+    detail::check(ctx_.handle(),
+                  sfntt_cm31_ntt(ctx_.handle(), inverse ? 1 : 0, pairs.data(), pairs.size(), log_n, batch, out.data(),
+                                 &ns),
+                  pairs.size());
+    return {std::move(out), ns};
+  }
+
+ private:
+  Context ctx_;
+};
+
 // ---- output layout ------------------------------------------------------------
 // Row order / row-major form of a SoA batch: SFNTT_LAYOUT_NATURAL (bit-reversed
 // rows -> natural), SFNTT_LAYOUT_ROW_MAJOR (out[row * batch + col], the

@@ -249,6 +249,29 @@ void check_koalabear(const sfntt::Context& ctx) {
           "KbCosetLdeBatch %s log_n 14 batch 3 added 2", fused ? "fused" : "unfused");
 }
 
+// Circle LDE and CM31 transforms (no reference counterpart) against the oracle.
+void check_circle_and_cm31(const sfntt::Context& ctx) {
+  const uint32_t log_n = 14, batch = 3, added = 1;
+  std::vector<uint32_t> x(size_t(batch) << log_n), ref(size_t(batch) << (log_n + added));
+  orc_lcg_fill(x.data(), x.size(), 5, ORC_M31_P, 0);
+  orc_circle_lde(x.data(), ref.data(), log_n, batch, added, 4);
+  sfntt::CircleLde circle(ctx);
+  CHECK(circle.execute(x, log_n, batch, added).data == ref, "CircleLde log_n 14 batch 3 added 1");
+  std::vector<uint32_t> ev = x;
+  orc_circle_ntt(ev.data(), log_n, batch, 0);
+  auto [got, ns] = circle.ntt(x, log_n, batch, false);
+  CHECK(got == ev, "CircleLde::ntt evaluate");
+  CHECK(circle.ntt(got, log_n, batch, true).first == x, "CircleLde::ntt interpolate(evaluate)");
+  std::vector<uint32_t> p(2 * (size_t(batch) << 10));
+  orc_lcg_fill(p.data(), p.size(), 6, ORC_M31_P, 0);
+  std::vector<uint32_t> pref = p;
+  orc_cm31_ntt(pref.data(), 10, batch, 0);
+  sfntt::Cm31Ntt cm(ctx);
+  auto [cf, ns2] = cm.ntt(p, 10, batch, false);
+  CHECK(cf == pref, "Cm31Ntt forward log_n 10 batch 3");
+  CHECK(cm.ntt(cf, 10, batch, true).first == p, "Cm31Ntt inverse(forward)");
+}
+
 int main(int argc, char** argv) {
   const bool no_device = argc > 1 && std::strcmp(argv[1], "--no-device") == 0;
   if (no_device) {
@@ -285,6 +308,7 @@ int main(int argc, char** argv) {
     check_pointwise_and_batch(ctx);
     check_lde(ctx);
     check_koalabear(ctx);
+    check_circle_and_cm31(ctx);
     check_layout(ctx);
     check_server(ctx);
   }
