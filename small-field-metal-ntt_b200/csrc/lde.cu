@@ -276,11 +276,14 @@ Status monty_lde_natural2x(sfntt_ctx* ctx, const uint32_t* d_in, uint32_t* d_out
   TmaRequest si{};
   si.in = d_in; si.out = mid; si.in_stride = n; si.out_stride = n; si.tw = itw;
   si.log_n = log_n; si.lo = 12; si.P = (int)log_n - 12; si.contiguous = false; si.batch = batch;
+  // a chunk's twiddles are staged once for its `batch` tiles (one per column)
+  si.lstage = batch >= 8;
   SFNTT_TRY(run_tma_pass_field(ctx, field, true, si, s));
   SFNTT_TRY(launch_tma_expand_c<F>(ctx, mid, d_out, log_n, batch, itw, ftw, mul, s));
   TmaRequest sf{};
   sf.in = d_out; sf.out = d_out; sf.in_stride = 2 * n; sf.out_stride = 2 * n; sf.tw = ctw;
   sf.log_n = log_n + 1; sf.lo = 13; sf.P = (int)log_n - 12; sf.contiguous = false; sf.batch = batch;
+  sf.lstage = batch >= 8;
   SFNTT_TRY(run_tma_pass_field(ctx, field, false, sf, s));
   *done = true;
   return {};

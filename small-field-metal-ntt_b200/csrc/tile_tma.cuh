@@ -89,6 +89,9 @@ struct TileCoord {
 template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false, bool LSTAGE = false>
 struct TPass {
   static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN), "chunk staging: BabyBear strided only");
+  // the staged lookup takes the lane part of a position from the thread alone:
+  // with P = 8 every slot bit of both rounds is a layer bit above the lanes
+  static_assert(!LSTAGE || P == 8, "chunk staging: 8-layer strided tiles");
   static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
   static constexpr int CB = P + LT;
   static constexpr int R = 4;
@@ -114,6 +117,18 @@ struct TPass {
         g.c1 = (int32_t)(r << (CB - 5));
         g.c2 = (int32_t)(t >> a.log_tpc);
       }
+    } else if constexpr (LSTAGE) {
+      // chunk slowest, then high block, then column: a CTA's contiguous range
+      // of tiles shares one 32-position chunk (and its twiddles) for
+      // batch * 2^(log_n - lo - P) tiles
+      const uint32_t per_chunk = a.batch << (a.log_n - a.lo - P);
+      const uint32_t lchunk = t / per_chunk;
+      const uint32_t r = t - lchunk * per_chunk;
+      g.hb = r / a.batch;
+      g.pos_base = lchunk << 5;
+      g.s1 = (int32_t)lchunk;
+      g.s3 = (int32_t)g.hb;
+      g.s4 = (int32_t)(r - g.hb * a.batch);
     } else {
       const uint32_t tt = t / a.batch;
       const uint32_t col = t - tt * a.batch;
@@ -453,8 +468,18 @@ struct TPass {
     uint2* tws = reinterpret_cast<uint2*>(bar + 2);
     const uint32_t tid = threadIdx.x;
     const TmaArgs& a = args;
-    uint32_t t = blockIdx.x;
-    if (t >= a.ntiles) return;
+    uint32_t t, t_end, t_step;
+    if constexpr (LSTAGE) {  // contiguous range per CTA
+      const uint32_t per = (a.ntiles + gridDim.x - 1) / gridDim.x;
+      t = blockIdx.x * per;
+      t_end = (t + per < a.ntiles) ? t + per : a.ntiles;
+      t_step = 1;
+    } else {
+      t = blockIdx.x;
+      t_end = a.ntiles;
+      t_step = gridDim.x;
+    }
+    if (t >= t_end) return;
     if constexpr (kStaged) stage_twiddles(tws, a.tw, tid);
     if (tid == 0) {
       tma::prefetch_map(min);
@@ -469,21 +494,32 @@ struct TPass {
       tma_load(min, geo(a, t), stage, &bar[0]);
     }
     uint32_t v[E];
-    for (uint32_t it = 0; t < a.ntiles; t += gridDim.x, ++it) {
+    uint32_t staged = ~0u;  // chunk whose twiddles are in shared memory (LSTAGE)
+    for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
       const uint32_t buf = it & 1u;
       uint32_t* cur = stage + buf * TWORDS;
-      const uint32_t tn = t + gridDim.x;
-      if (tid == 0 && tn < a.ntiles) {
+      const uint32_t tn = t + t_step;
+      if (tid == 0 && tn < t_end) {
         tma::wait_reads();  // the store that last used the other buffer has read it
         tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
         tma_load(min, geo(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+      }
+      const Geo g = geo(a, t);
+      if constexpr (LSTAGE) {
+        // Every thread passed the previous tile's pre-store barrier after its
+        // last twiddle read; the barrier here publishes the new copy (the
+        // chunk is a function of t, the same for the whole CTA).
+        if ((uint32_t)g.s1 != staged) {
+          stage_lchunk(tws, a.tw, a.lo, (uint32_t)g.s1, tid);
+          staged = (uint32_t)g.s1;
+          __syncthreads();
+        }
       }
       // A wait that ran out is agreed on at the barrier before the store:
       // the rounds in between touch only in-bounds shared memory and
       // twiddles whatever the tile holds, and every thread takes the same
       // barriers, so no extra CTA-wide barrier is needed per tile.
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
-      const Geo g = geo(a, t);
       ld<kFirst>(cur, v, tid);
       if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
       rounds<0>(cur, v, a, tws, g, tid);
@@ -493,7 +529,7 @@ struct TPass {
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(a.err, 1);
-          if (tn < a.ntiles) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
           tma::wait_all();
         }
         return;
@@ -514,11 +550,13 @@ static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<1, 0>() == 0x1F0, "C12 
 static_assert(TPass<BabyBear, false, Kind::C, 8>::xfixed<0, 1>() == 0x1F0, "C8 0->1: in a warp");
 static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: lanes only, whole CTA");
 
-template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
-__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW>::NT, 2)
+// LSTAGE passes stage 32 (2^P - 1) twiddle pairs (64 KiB for P = 8) besides
+// the two tiles: one CTA per SM.
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false>
+__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::NT, LSTAGE ? 1 : 2)
 tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
   pdl_enter();
-  TPass<F, DESC, KD, P, PLAIN, TW>::run(&min, &mout, a);
+  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::run(&min, &mout, a);
 }
 
 // ---------------------------------------------------------------------------

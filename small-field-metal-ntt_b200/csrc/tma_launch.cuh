@@ -24,6 +24,7 @@ struct TmaRequest {
   const uint2* twist = nullptr;  // BabyBear four-step twist at the boundary
   uint32_t twist_mask = 0;
   bool plain = false;            // BabyBear strided pass: plain sub-transform (twist by neighbours)
+  bool lstage = false;           // BabyBear 8-layer strided pass: per-chunk twiddles staged in shared memory
 };
 
 // Resolved once through the runtime (no link-time dependency on libcuda).
@@ -71,17 +72,17 @@ inline Status encode_s_map(CUtensorMap* m, const uint32_t* base, uint32_t lo, in
   return tensor_map_encode(m, base, 5, dims, strides, box);
 }
 
-template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE>
 const char* tma_pass_name() {
   static const std::string nm = std::string(F::kTag) + "_" + (DESC ? "fwd" : "inv") +
                                 "_tma_" + (KD == Kind::C ? "C" : "S") + std::to_string(P) + (PLAIN ? "p" : "") +
-                                (TW ? "t" : "");
+                                (TW ? "t" : "") + (LSTAGE ? "c" : "");
   return nm.c_str();
 }
 
-template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false>
 Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
-  using T = TPass<F, DESC, KD, P, PLAIN, TW>;
+  using T = TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
   const uint64_t n = 1ull << r.log_n;
   CUtensorMap min, mout;
   TmaArgs a{};
@@ -109,14 +110,15 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
   }
-  constexpr int smem = 2 * (int)T::TBYTES + 16 + 8 * (int)T::TW_ENTRIES + 1024;
-  auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW>;
+  constexpr int smem = 2 * (int)T::TBYTES + 16 + 8 * (int)(LSTAGE ? T::LCHUNK_ENTRIES : T::TW_ENTRIES) + 1024;
+  auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
-  const uint32_t grid = std::min<uint32_t>(a.ntiles, 2u * (uint32_t)ctx->sm_count);
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, (LSTAGE ? 1u : 2u) * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   SFNTT_CU(launch_pdl(kern, grid, T::NT, smem, s, pdl_fits(grid), min, mout, a));
-  return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW>(), s, ((uint64_t)r.batch << r.log_n) * 8u);
+  return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW, LSTAGE>(), s,
+                      ((uint64_t)r.batch << r.log_n) * 8u);
 }
 
 // BabyBear and KoalaBear instantiate the twist / plain variants; M31 never needs them.
@@ -132,6 +134,9 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
       if (r.plain && r.twist) return launch_tma_pass<F, DESC, Kind::S, PP, true, true>(ctx, r, s); \
       if (r.plain) return launch_tma_pass<F, DESC, Kind::S, PP, true, false>(ctx, r, s);         \
       if (r.twist) return launch_tma_pass<F, DESC, Kind::S, PP, false, true>(ctx, r, s);         \
+      if constexpr (PP == 8) {                                                                   \
+        if (r.lstage) return launch_tma_pass<F, DESC, Kind::S, PP, false, false, true>(ctx, r, s); \
+      }                                                                                          \
     }                                                                                            \
     return launch_tma_pass<F, DESC, Kind::S, PP, false, false>(ctx, r, s);
 

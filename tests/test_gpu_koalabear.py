@@ -115,6 +115,20 @@ def test_kb_coset_lde_generator_shift_and_natural(ctx):
     assert np.array_equal(nat.reshape(batch, n_ext), r.data.reshape(batch, n_ext)[:, rev(log_n + added)])
 
 
+def test_kb_natural_lde_full_size_sampled_columns(ctx):
+    """2^20 x 8 natural-order rows (the mirrored network, strided passes with
+    chunk-staged twiddles): sampled columns against the oracle."""
+    log_n, batch, added = 20, 8, 1
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    rev = lambda bits: np.array([int(format(k, f"0{bits}b")[::-1], 2) for k in range(1 << bits)])
+    r_n, r_ext = rev(log_n), rev(log_n + added)
+    x_nat = kdata(batch << log_n, 2027)
+    got = sfntt.KbCosetLdeBatch(ctx, natural=True).execute(x_nat, log_n, batch, added).data.reshape(batch, n_ext)
+    for c in (0, 3, batch - 1):
+        ref = O.kb_coset_lde(x_nat[c * n:(c + 1) * n][r_n], log_n, 1, added)
+        assert np.array_equal(got[c], ref[r_ext]), c
+
+
 def test_kb_coset_lde_full_size_sampled_columns(ctx):
     """2^20 x 64, 2x: sampled columns against the oracle; the extension
     interpolates to a polynomial of degree < n on every column."""
