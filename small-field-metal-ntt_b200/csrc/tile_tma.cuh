@@ -88,10 +88,16 @@ struct TileCoord {
 // shared-memory load instead of an L2 one.
 template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false, bool LSTAGE = false>
 struct TPass {
-  static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN), "chunk staging: BabyBear strided only");
-  // the staged lookup takes the lane part of a position from the thread alone:
-  // with P = 8 every slot bit of both rounds is a layer bit above the lanes
-  static_assert(!LSTAGE || P == 8, "chunk staging: 8-layer strided tiles");
+  // LSTAGE: each CTA takes a contiguous range of tiles ordered so that it
+  // stays on one set of positions across the columns, and stages that set's
+  // twiddles in shared memory.  BabyBear strided tiles: the per-position
+  // twiddles of a 32-position chunk (the staged lookup takes the lane part of
+  // a position from the thread alone: with P = 8 every slot bit of both rounds
+  // is a layer bit above the lanes).  M31 12-layer contiguous tiles: the
+  // per-block twiddles of the tile's 2^13 positions.
+  static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN && P == 8) ||
+                    (KD == Kind::C && !F::kMontgomery && P == 12 && !TW),
+                "position staging: BabyBear 8-layer strided or M31 12-layer contiguous tiles");
   static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
   static constexpr int CB = P + LT;
   static constexpr int R = 4;
@@ -112,10 +118,17 @@ struct TPass {
         g.c1 = (int32_t)(t << (CB - 5));
         g.c2 = 0;
       } else {
-        const uint32_t r = t & ((1u << a.log_tpc) - 1u);
+        uint32_t r, col;
+        if constexpr (LSTAGE) {  // column fastest: consecutive tiles share their positions
+          r = t / a.batch;
+          col = t - r * a.batch;
+        } else {
+          r = t & ((1u << a.log_tpc) - 1u);
+          col = t >> a.log_tpc;
+        }
         g.pos_base = r << CB;
         g.c1 = (int32_t)(r << (CB - 5));
-        g.c2 = (int32_t)(t >> a.log_tpc);
+        g.c2 = (int32_t)col;
       }
     } else if constexpr (LSTAGE) {
       // chunk slowest, then high block, then column: a CTA's contiguous range
@@ -169,7 +182,37 @@ struct TPass {
            mp.ngrp == 1 && mp.gshift[0] == 4 && mp.gmask[0] == (1u << (kTileBits - 4)) - 1u;
   }
   static constexpr bool kRound0Copy = !F::kMontgomery && KD == Kind::C && round0_linear();
+  static_assert(!LSTAGE || KD == Kind::S || kRound0Copy, "M31 tile staging starts from the first-round copy");
   static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
+  // M31 tile staging: the twiddles of a tile's 2^13 positions, one word each
+  // (the Shoup companion is recomputed, m31_shoup_of), laid out like a
+  // 2^13-point table with layer L at 8192 - (8192 >> L); layers 0..3 (words
+  // [0, 7680)) are ordered by thread: layer j gives thread t its 2^(3-j)
+  // twiddles as vectors of v = min(2^(3-j), 4) words at v (g NT + t), group g.
+  static constexpr uint32_t CTILE_ENTRIES = 8190u;
+  // staged twiddle bytes in shared memory, CTAs per SM
+  static constexpr uint32_t SMEM_TW_BYTES =
+      LSTAGE ? (KD == Kind::S ? 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
+  static constexpr int kCtasPerSm = (LSTAGE && KD == Kind::S) ? 1 : 2;
+
+  // C = 1, 2 or 4 consecutive staged M31 twiddles from shared memory (p
+  // aligned to C words) into tv[AT, AT + C), with their Shoup companions
+  template <int C, int AT>
+  __device__ static __forceinline__ void staged_w(const uint32_t* p, uint2 (&tv)[E / 2]) {
+    uint32_t w[4];
+    if constexpr (C == 1) {
+      w[0] = p[0];
+    } else if constexpr (C == 2) {
+      const uint2 q = *reinterpret_cast<const uint2*>(p);
+      w[0] = q.x; w[1] = q.y;
+    } else {
+      static_assert(C == 4, "one vector load");
+      const uint4 q = *reinterpret_cast<const uint4*>(p);
+      w[0] = q.x; w[1] = q.y; w[2] = q.z; w[3] = q.w;
+    }
+#pragma unroll
+    for (int i = 0; i < C; ++i) tv[AT + i] = make_uint2(w[i], m31_shoup_of(w[i]));
+  }
 
   // ---- twiddles: per-layer base pointer + compile-time offset per slot ----
   template <int k>
@@ -183,7 +226,7 @@ struct TPass {
       const uint32_t mask = (1u << beta) - 1u;
       if constexpr (KD == Kind::C) return base[(ct & mask) + (cm & mask)];
       else return base[((ct >> 5) & mask) + ((cm >> 5) & mask)];
-    } else if constexpr (LSTAGE) {  // tw[L][pos mod 2^L] from the chunk's staged copy
+    } else if constexpr (LSTAGE && KD == Kind::S) {  // tw[L][pos mod 2^L] from the chunk's staged copy
       const uint32_t em = (1u << beta) - 1u;
       return tws[32u * em + ((((ct >> 5) & em) + ((cm >> 5) & em)) << 5) + (ct & 31u)];
     } else if constexpr (F::kMontgomery) {  // BabyBear strided, per position: tw[L][pos mod 2^L]
@@ -222,37 +265,58 @@ struct TPass {
         const uint32_t L = a.lo + beta;
         const uint32_t n = 1u << a.log_n;
         uint2 tv[E / 2];
-        bool copied = false;
-        if constexpr (kRound0Copy && k == 0) {
-          if (a.tw0) {
-            // the table's first-round copy: [tile][layer][pair][thread], coalesced across the CTA
-            const uint2* t0 = a.tw0 + (g.pos_base >> 13) * 7680u;
-            const uint32_t off = j == 0 ? 0u : j == 1 ? 4096u : j == 2 ? 6144u : 7168u;
+        if constexpr (LSTAGE) {
+          // this thread's 2^(r-1-j) twiddles of layer j (a constant once unrolled)
+          const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (8192u - (8192u >> L));
+          if constexpr (k == 0) {  // thread-ordered first-round layers
+            switch (r - 1 - j) {
+              case 3: staged_w<4, 0>(tw32 + 4u * tid, tv); staged_w<4, 4>(tw32 + 4u * (NT + tid), tv); break;
+              case 2: staged_w<4, 0>(tw32 + 4u * tid, tv); break;
+              case 1: staged_w<2, 0>(tw32 + 2u * tid, tv); break;
+              default: staged_w<1, 0>(tw32 + tid, tv); break;
+            }
+          } else {
+            const uint32_t* p = tw32 + (ct >> (L + 1));
+            switch (r - 1 - j) {
+              case 3: staged_w<4, 0>(p, tv); staged_w<4, 4>(p + 4, tv); break;
+              case 2: staged_w<4, 0>(p, tv); break;
+              case 1: staged_w<2, 0>(p, tv); break;
+              default: staged_w<1, 0>(p, tv); break;
+            }
+          }
+        } else {
+          bool copied = false;
+          if constexpr (kRound0Copy && k == 0) {
+            if (a.tw0) {
+              // the table's first-round copy: [tile][layer][pair][thread], coalesced across the CTA
+              const uint2* t0 = a.tw0 + (g.pos_base >> 13) * 7680u;
+              const uint32_t off = j == 0 ? 0u : j == 1 ? 4096u : j == 2 ? 6144u : 7168u;
+              if (j == r - 1) {
+                tv[0] = __ldg(t0 + off + tid);
+              } else {
+#pragma unroll
+                for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
+                  const uint4 q = __ldg(reinterpret_cast<const uint4*>(t0 + off) + (uint32_t)(o >> 1) * NT + tid);
+                  tv[o] = make_uint2(q.x, q.y);
+                  tv[o + 1] = make_uint2(q.z, q.w);
+                }
+              }
+              copied = true;
+            }
+          }
+          if (!copied) {
+            const uint2* base = a.tw + (n - (n >> L));
+            if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1));
+            else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
             if (j == r - 1) {
-              tv[0] = __ldg(t0 + off + tid);
+              tv[0] = __ldg(base);
             } else {
 #pragma unroll
               for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
-                const uint4 q = __ldg(reinterpret_cast<const uint4*>(t0 + off) + (uint32_t)(o >> 1) * NT + tid);
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(base + o));
                 tv[o] = make_uint2(q.x, q.y);
                 tv[o + 1] = make_uint2(q.z, q.w);
               }
-            }
-            copied = true;
-          }
-        }
-        if (!copied) {
-          const uint2* base = a.tw + (n - (n >> L));
-          if constexpr (KD == Kind::C) base += (g.pos_base >> (L + 1)) + ((ct & (n - 1u)) >> (L + 1));
-          else base += (g.hb << (P - beta - 1)) + ((ct >> 5) >> (beta + 1));
-          if (j == r - 1) {
-            tv[0] = __ldg(base);
-          } else {
-#pragma unroll
-            for (int o = 0; o < (1 << (r - 1 - j)); o += 2) {
-              const uint4 q = __ldg(reinterpret_cast<const uint4*>(base + o));
-              tv[o] = make_uint2(q.x, q.y);
-              tv[o + 1] = make_uint2(q.z, q.w);
             }
           }
         }
@@ -459,6 +523,31 @@ struct TPass {
     }
   }
 
+  // M31 per-block twiddles (first words) of the 12 layers over tile positions
+  // [pos_base, pos_base + 2^13): layers 0..3 from the table's first-round
+  // copy ([layer][pair group][thread], a pair group = two pairs), layers
+  // 4..11 from the table (2^(12-L) consecutive entries each).
+  __device__ static __forceinline__ void stage_ctile(uint32_t* dst, const TmaArgs& a, uint32_t pos_base,
+                                                     uint32_t tid) {
+    const uint2* src0 = a.tw0 + (pos_base >> 13) * 7680u;
+    for (uint32_t d = tid; d < 7680u; d += NT) {
+      const uint32_t j = d < 4096u ? 0u : d < 6144u ? 1u : d < 7168u ? 2u : 3u;
+      const uint32_t off = 8192u - (8192u >> j);
+      const uint32_t rel = d - off;
+      const uint32_t v = j <= 1u ? 4u : (j == 2u ? 2u : 1u);
+      const uint32_t t = (rel / v) & (NT - 1u);
+      const uint32_t o = (rel / (v * NT)) * v + (rel & (v - 1u));  // the thread's o-th twiddle of layer j
+      const uint32_t sp = j == 3u ? off + t : off + 2u * ((o >> 1) * NT + t) + (o & 1u);
+      dst[d] = __ldg(&src0[sp].x);
+    }
+    const uint32_t n = 1u << a.log_n;
+    for (uint32_t e = 7680u + tid; e < CTILE_ENTRIES; e += NT) {
+      const uint32_t L = 12u - (31u - __clz(8191u - e));  // e in [8192 - 2^(13-L), 8192 - 2^(12-L))
+      const uint32_t local = e - (8192u - (8192u >> L));
+      dst[e] = __ldg(&a.tw[(n - (n >> L)) + (pos_base >> (L + 1)) + local].x);
+    }
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
@@ -508,10 +597,12 @@ struct TPass {
       if constexpr (LSTAGE) {
         // Every thread passed the previous tile's pre-store barrier after its
         // last twiddle read; the barrier here publishes the new copy (the
-        // chunk is a function of t, the same for the whole CTA).
-        if ((uint32_t)g.s1 != staged) {
-          stage_lchunk(tws, a.tw, a.lo, (uint32_t)g.s1, tid);
-          staged = (uint32_t)g.s1;
+        // positions are a function of t, the same for the whole CTA).
+        const uint32_t key = (KD == Kind::C) ? g.pos_base : (uint32_t)g.s1;
+        if (key != staged) {
+          if constexpr (KD == Kind::C) stage_ctile(reinterpret_cast<uint32_t*>(tws), a, g.pos_base, tid);
+          else stage_lchunk(tws, a.tw, a.lo, (uint32_t)g.s1, tid);
+          staged = key;
           __syncthreads();
         }
       }
@@ -550,10 +641,11 @@ static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<1, 0>() == 0x1F0, "C12 
 static_assert(TPass<BabyBear, false, Kind::C, 8>::xfixed<0, 1>() == 0x1F0, "C8 0->1: in a warp");
 static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: lanes only, whole CTA");
 
-// LSTAGE passes stage 32 (2^P - 1) twiddle pairs (64 KiB for P = 8) besides
-// the two tiles: one CTA per SM.
+// BabyBear LSTAGE passes stage 64 KiB of twiddles besides the two tiles (one
+// CTA per SM); M31 contiguous ones 32 KiB (two).
 template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false>
-__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::NT, LSTAGE ? 1 : 2)
+__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::NT,
+                                  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::kCtasPerSm)
 tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
   pdl_enter();
   TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::run(&min, &mout, a);

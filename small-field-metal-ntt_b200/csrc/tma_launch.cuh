@@ -24,7 +24,9 @@ struct TmaRequest {
   const uint2* twist = nullptr;  // BabyBear four-step twist at the boundary
   uint32_t twist_mask = 0;
   bool plain = false;            // BabyBear strided pass: plain sub-transform (twist by neighbours)
-  bool lstage = false;           // BabyBear 8-layer strided pass: per-chunk twiddles staged in shared memory
+  // per-position twiddles staged in shared memory, one CTA per SM walking the
+  // columns (BabyBear 8-layer strided or M31 12-layer contiguous passes, n >= 2^13)
+  bool lstage = false;
 };
 
 // Resolved once through the runtime (no link-time dependency on libcuda).
@@ -110,11 +112,11 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
   }
-  constexpr int smem = 2 * (int)T::TBYTES + 16 + 8 * (int)(LSTAGE ? T::LCHUNK_ENTRIES : T::TW_ENTRIES) + 1024;
+  constexpr int smem = 2 * (int)T::TBYTES + 16 + (int)T::SMEM_TW_BYTES + 1024;
   auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
-  const uint32_t grid = std::min<uint32_t>(a.ntiles, (LSTAGE ? 1u : 2u) * (uint32_t)ctx->sm_count);
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)T::kCtasPerSm * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   SFNTT_CU(launch_pdl(kern, grid, T::NT, smem, s, pdl_fits(grid), min, mout, a));
   return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW, LSTAGE>(), s,
@@ -126,6 +128,9 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   case PP:                                                                                       \
     if constexpr (F::kMontgomery) {                                                              \
       if (r.twist) return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);         \
+    } else if constexpr (PP == 12) {                                                             \
+      if (r.lstage && r.log_n >= kTileBits)                                                      \
+        return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);             \
     }                                                                                            \
     return launch_tma_pass<F, DESC, Kind::C, PP, false, false>(ctx, r, s);
 #define SFNTT_TMA_S(PP)                                                                          \

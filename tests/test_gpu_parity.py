@@ -304,6 +304,33 @@ def test_m31_lde_full_size_sampled_columns(ctx):
     assert np.array_equal(ext[:, :n], base.reshape(batch, n))
 
 
+@pytest.mark.parametrize("log_n,batch", [(16, 19), (13, 16), (14, 33)])
+def test_m31_batch_staged_tile_twiddles(ctx, log_n, batch):
+    """M31 12-layer contiguous passes over >= 16 columns stage each tile's
+    twiddles once for all of its columns (tiles column-fastest, a CTA's range
+    crossing tile positions at odd column counts): every column against the
+    oracle, and the round trip."""
+    b = sfntt.CudaCtGsR4(ctx)
+    x = data(M31, batch << log_n, 900 + log_n)
+    fw, _ = b.forward_ntt_batch_gpu(x, log_n, batch)
+    n = 1 << log_n
+    for c in range(batch):
+        assert np.array_equal(fw[c * n:(c + 1) * n], O.m31_forward(x[c * n:(c + 1) * n])), c
+    back, _ = b.inverse_ntt_batch_gpu(fw, log_n, batch)
+    assert np.array_equal(back, x)
+
+
+def test_m31_lde_staged_odd_columns(ctx):
+    """M31 blow-up 2^20 x 17: the staged contiguous passes with tile ranges
+    that change position inside a CTA; sampled columns against the oracle."""
+    log_n, batch, added = 20, 17, 1
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    x = O.lcg(batch << log_n, 1717, O.M31_P)
+    r = sfntt.M31Lde(ctx).execute(x, log_n, batch, added)
+    for c in (0, 8, batch - 1):
+        assert np.array_equal(r.data[c * n_ext:(c + 1) * n_ext], O.m31_lde(x[c * n:(c + 1) * n], log_n, 1, added)), c
+
+
 def test_extension_size_cannot_wrap(ctx):
     """log_n + added_bits is range-checked before it is summed in 32 bits:
     an added_bits near 2^32 must not wrap into a small, accepted size."""
