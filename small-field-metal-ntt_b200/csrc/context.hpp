@@ -114,6 +114,8 @@ struct sfntt_ctx {
   sfntt::DevBuf err;
   // route every pass through the first (non-TMA) tile engine (tests / A-B)
   bool no_tma = false;
+  // single-launch cluster NTT for columns of 2^13 .. 2^16 points off (A-B)
+  bool no_cluster = false;
   // BabyBear strided passes: plain sub-transforms + four-step twists applied by
   // neighbouring passes (true) or per-position twiddles (false); separately
   // for plain NTTs and the fused LDE.
@@ -179,6 +181,12 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
                   uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
                   const uint2* tw, cudaStream_t stream, const uint2* edge_twist = nullptr,
                   uint32_t edge_mask = 0);
+// One-launch NTT of 2^13 .. 2^16-point columns on a thread-block cluster
+// (cluster_ntt.cu), in place on dense columns; fits: shape, alignment and at
+// most one wave of CTAs.
+bool cluster_ntt_fits(const sfntt_ctx* ctx, uint32_t log_n, uint32_t batch, const void* d);
+Status cluster_ntt_dev(sfntt_ctx* ctx, int field, bool inverse, uint32_t* d, uint32_t log_n, uint32_t batch,
+                       const uint2* tw, uint32_t scale_w, cudaStream_t stream);
 Status ntt_dev_oop(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* d_in, uint32_t* d_out,
                    uint64_t in_stride, uint64_t out_stride, uint32_t log_n, uint32_t batch, bool normalize,
                    cudaStream_t stream);

@@ -240,6 +240,10 @@ Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d
       return {};
     }
     default:
+      // 2^13 .. 2^16 points in at most one wave of CTAs: one cluster launch
+      // instead of two passes
+      if (!ctx->no_tma && cluster_ntt_fits(ctx, log_n, batch, d))
+        return cluster_ntt_dev(ctx, field, inverse, d, log_n, batch, tw, scale, s);
       return layers_dev(ctx, field, inverse, d, d, stride, stride, log_n, batch, 0, log_n, scale, tw, s);
   }
 }
