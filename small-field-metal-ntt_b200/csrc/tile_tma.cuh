@@ -110,6 +110,8 @@ struct TPass {
 
   using Geo = TileCoord;
 
+  // Tile t of a pass: Kind::C position-fastest, Kind::S column-fastest, then
+  // chunk, then high block.
   __device__ static __forceinline__ Geo geo(const TmaArgs& a, uint32_t t) {
     Geo g{};
     if constexpr (KD == Kind::C) {
@@ -118,30 +120,11 @@ struct TPass {
         g.c1 = (int32_t)(t << (CB - 5));
         g.c2 = 0;
       } else {
-        uint32_t r, col;
-        if constexpr (LSTAGE) {  // column fastest: consecutive tiles share their positions
-          r = t / a.batch;
-          col = t - r * a.batch;
-        } else {
-          r = t & ((1u << a.log_tpc) - 1u);
-          col = t >> a.log_tpc;
-        }
+        const uint32_t r = t & ((1u << a.log_tpc) - 1u);
         g.pos_base = r << CB;
         g.c1 = (int32_t)(r << (CB - 5));
-        g.c2 = (int32_t)col;
+        g.c2 = (int32_t)(t >> a.log_tpc);
       }
-    } else if constexpr (LSTAGE) {
-      // chunk slowest, then high block, then column: a CTA's contiguous range
-      // of tiles shares one 32-position chunk (and its twiddles) for
-      // batch * 2^(log_n - lo - P) tiles
-      const uint32_t per_chunk = a.batch << (a.log_n - a.lo - P);
-      const uint32_t lchunk = t / per_chunk;
-      const uint32_t r = t - lchunk * per_chunk;
-      g.hb = r / a.batch;
-      g.pos_base = lchunk << 5;
-      g.s1 = (int32_t)lchunk;
-      g.s3 = (int32_t)g.hb;
-      g.s4 = (int32_t)(r - g.hb * a.batch);
     } else {
       const uint32_t tt = t / a.batch;
       const uint32_t col = t - tt * a.batch;
@@ -154,6 +137,34 @@ struct TPass {
       g.s4 = (int32_t)col;
     }
     return g;
+  }
+
+  // The tile order of run(): geo's, except that LSTAGE passes keep a set of
+  // positions across the columns -- Kind::C column-fastest; Kind::S chunk
+  // slowest, then high block, then column -- so a CTA's contiguous range of
+  // tiles shares one staged copy of twiddles for batch (x high blocks) tiles.
+  __device__ static __forceinline__ Geo geo_run(const TmaArgs& a, uint32_t t) {
+    if constexpr (!LSTAGE) {
+      return geo(a, t);
+    } else {
+      Geo g{};
+      if constexpr (KD == Kind::C) {  // n >= 2^13 (never spanning)
+        const uint32_t r = t / a.batch;
+        g.pos_base = r << CB;
+        g.c1 = (int32_t)(r << (CB - 5));
+        g.c2 = (int32_t)(t - r * a.batch);
+      } else {
+        const uint32_t per_chunk = a.batch << (a.log_n - a.lo - P);
+        const uint32_t lchunk = t / per_chunk;
+        const uint32_t r = t - lchunk * per_chunk;
+        g.hb = r / a.batch;
+        g.pos_base = lchunk << 5;
+        g.s1 = (int32_t)lchunk;
+        g.s3 = (int32_t)g.hb;
+        g.s4 = (int32_t)(r - g.hb * a.batch);
+      }
+      return g;
+    }
   }
 
   __device__ static __forceinline__ void tma_load(const CUtensorMap* m, const Geo& g, uint32_t* dst, uint64_t* bar) {
@@ -580,7 +591,7 @@ struct TPass {
     __syncthreads();
     if (tid == 0) {
       tma::mbar_expect_tx(&bar[0], TBYTES);
-      tma_load(min, geo(a, t), stage, &bar[0]);
+      tma_load(min, geo_run(a, t), stage, &bar[0]);
     }
     uint32_t v[E];
     uint32_t staged = ~0u;  // chunk whose twiddles are in shared memory (LSTAGE)
@@ -591,9 +602,9 @@ struct TPass {
       if (tid == 0 && tn < t_end) {
         tma::wait_reads();  // the store that last used the other buffer has read it
         tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
-        tma_load(min, geo(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+        tma_load(min, geo_run(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
       }
-      const Geo g = geo(a, t);
+      const Geo g = geo_run(a, t);
       if constexpr (LSTAGE) {
         // Every thread passed the previous tile's pre-store barrier after its
         // last twiddle read; the barrier here publishes the new copy (the
