@@ -66,8 +66,9 @@ def parse():
     ap.add_argument("--slots", type=int, default=8, help="served stream: concurrent request slots")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="served stream: HBM admission budget")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table"],
-                    help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph")
+    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table", "ntt"],
+                    help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph; "
+                         "ntt: forward + inverse NTT pairs of --batch columns of 2^--log-n points (--field)")
     ap.add_argument("--lanes", type=int, default=8)
     return ap.parse_args()
 
@@ -274,9 +275,9 @@ def main() -> None:
     if a.impl == "reference":
         run_reference(a, rank)
         return
-    if a.workload in ("uneven", "served", "table"):
+    if a.workload in ("uneven", "served", "table", "ntt"):
         if rank == 0:  # single-GPU workloads: under torchrun the other ranks have no work
-            {"uneven": run_uneven, "served": run_served, "table": run_table}[a.workload](a)
+            {"uneven": run_uneven, "served": run_served, "table": run_table, "ntt": run_ntt}[a.workload](a)
         return
 
     import torch
@@ -553,6 +554,65 @@ def run_served(a) -> None:
     line = {"metric": "served stream p50/p99 and Melem/s vs plain loop", "unit": "Melem/s",
             "value": top["served_melem_s"], "higher_is_better": True, "plain_loop_melem_s": top["plain_melem_s"],
             "served": res, "data": "synthetic", "device": ctx.device_info()}
+    print(json.dumps(line), flush=True)
+
+
+def run_ntt(a) -> None:
+    """Forward + inverse NTT pairs (the single-column configurations: M31
+    2^16, BabyBear 2^10..2^24) on device-resident columns: 10 pairs captured
+    in a CUDA graph, replayed --steps times after --warmup plain pairs; then
+    the per-kernel device times of 10 more pairs."""
+    import torch
+    import sfntt
+    torch.cuda.set_device(0)
+    ctx = sfntt.Context(0)
+    field = {"bb": sfntt.FIELD_BABYBEAR, "m31": sfntt.FIELD_M31, "kb": sfntt.FIELD_KOALABEAR}[a.field]
+    backend = {"bb": sfntt.BbCudaCtGsR4, "m31": sfntt.CudaCtGsR4, "kb": sfntt.KbCudaCtGsR4}[a.field](ctx)
+    p = {"bb": BB_P, "m31": 2147483647, "kb": KB_P}[a.field]
+    log_n, cols = a.log_n, a.batch
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(2024)
+    d = torch.randint(0, p, (cols << log_n,), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    ptr = d.data_ptr()
+    ctx.prepare(field, log_n)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(max(a.warmup, 3)):
+        backend.forward_dev(ptr, log_n, cols, stream)
+        backend.inverse_dev(ptr, log_n, cols, stream)
+    torch.cuda.synchronize()
+    graph, per_graph = torch.cuda.CUDAGraph(), 10
+    with torch.cuda.graph(graph):
+        cs = torch.cuda.current_stream().cuda_stream
+        for _ in range(per_graph):
+            backend.forward_dev(ptr, log_n, cols, cs)
+            backend.inverse_dev(ptr, log_n, cols, cs)
+    graph.replay()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        graph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    del graph
+    us = e0.elapsed_time(e1) * 1e3 / (a.steps * per_graph)
+    ctx.kernel_timing(True)
+    for _ in range(per_graph):
+        backend.forward_dev(ptr, log_n, cols, stream)
+        backend.inverse_dev(ptr, log_n, cols, stream)
+    torch.cuda.synchronize()
+    kt = ctx.kernel_times()
+    ctx.kernel_timing(False)
+    elems = cols << log_n
+    peak, peak_kind = peaks()
+    line = {"metric": f"{a.field} NTT forward+inverse 2^{log_n} x {cols}", "value": us, "unit": "us",
+            "higher_is_better": False, "steps": a.steps, "warmup": a.warmup,
+            "gelem_s": 2 * elems / (us * 1e-6) / 1e9,
+            "hbm_frac": 16 * elems / (us * 1e-6) / 1e9 / peak, "peak_kind": peak_kind,
+            "kernels": {k: {"launches": v[0], "avg_us": 1e3 * v[1] / v[0]} for k, v in kt.items()},
+            "data": "synthetic: seeded uniform values in [0, p), device-resident",
+            "config": {"workload": f"{a.field} forward + inverse NTT, {cols} column(s) of 2^{log_n} points",
+                       "l2": "columns of up to 2^24 words stay resident in L2 (126 MB)"},
+            "device": ctx.device_info()}
     print(json.dumps(line), flush=True)
 
 
