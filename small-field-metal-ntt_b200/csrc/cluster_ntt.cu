@@ -13,9 +13,10 @@
 // group lives in CTA k >> 1 at word base + (k & 1) 2^12.
 //
 //   inverse (layers ascending): load the block, in-block layers, cluster
-//     barrier, gather the groups from the cluster's blocks, cluster barrier
-//     (no block leaves while others read it), cross layers and n^-1, store
-//     the groups (consecutive threads own consecutive bases: coalesced).
+//     barrier, gather the groups from the cluster's blocks, cross layers and
+//     n^-1, store the groups (consecutive threads own consecutive bases:
+//     coalesced); a second cluster barrier, split around the last two steps,
+//     keeps every block alive until the others have read it.
 //   forward (layers descending): load the groups, cross layers, scatter them
 //     into the owning blocks, cluster barrier, in-block layers, store the block.
 //
@@ -148,12 +149,16 @@ struct ClusterNtt {
           const uint32_t* owner = cluster.map_shared_rank(tile, (unsigned)(k >> 1));
           v[gi * G + k] = owner[TP::sw(base0 + (uint32_t)gi * NT + ((uint32_t)(k & 1) << 12))];
         }
-      cluster.sync();  // no block leaves while another still reads it
+      // No block may leave while another still reads it: arrive once the
+      // reads are performed (release), wait only before leaving, so the
+      // barrier overlaps the cross layers and the stores.
+      asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
       cross(v, base0, tw, scale_w, scale_ws);
 #pragma unroll
       for (int gi = 0; gi < GPT; ++gi)
 #pragma unroll
         for (int k = 0; k < G; ++k) col[base0 + (uint32_t)gi * NT + ((uint32_t)k << 12)] = v[gi * G + k];
+      asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     }
   }
 };
