@@ -685,6 +685,10 @@ struct TExpand {
   static constexpr uint32_t TWORDS = Inv::TWORDS, TBYTES = Inv::TBYTES;
   static constexpr uint32_t TW_ENTRIES = LSTAGE ? Inv::LCHUNK_ENTRIES : Inv::TW_ENTRIES;  // per direction
   static_assert(F::kMontgomery || !PLAIN, "M31 passes have no plain variant");
+  // M31 stages no twiddles (3 x 32 KiB of shared memory) and fits 64 registers:
+  // two CTAs per SM; BabyBear / KoalaBear keep their multipliers in registers
+  // one block ahead and stage twiddles, one CTA per SM.
+  static constexpr int kCtasPerSm = F::kMontgomery ? 1 : 2;
 
   // Multipliers M_q of the thread's 16 slots (round K-1 layout) from mq = M_q + pos_t.
   __device__ static __forceinline__ void load_mul(uint2 (&w)[E], const uint2* mq, uint32_t lo) {
@@ -957,7 +961,7 @@ tma_expand_c_kernel(const __grid_constant__ CUtensorMap min, const __grid_consta
 }
 
 template <class F, int P, bool PLAIN, bool LSTAGE>
-__global__ void __launch_bounds__(TExpand<F, P, PLAIN, LSTAGE>::NT, 1)
+__global__ void __launch_bounds__(TExpand<F, P, PLAIN, LSTAGE>::NT, TExpand<F, P, PLAIN, LSTAGE>::kCtasPerSm)
 tma_expand_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
   pdl_enter();
   TExpand<F, P, PLAIN, LSTAGE>::run(&min, &mout, a);
