@@ -74,6 +74,9 @@ typedef struct sfntt_ctx sfntt_ctx;
 
 /* ---- context: replaces MetalContext::new / backend ::new(shader_dir)
  *      (src/gpu.rs:26-64, src/ntt/babybear/metal_ct_gs_r4.rs:44-85). */
+/* Read once at creation, for comparisons: SFNTT_NO_TMA=1 routes every pass
+ * through the first (non-TMA) tile engine; SFNTT_NO_CLUSTER=1 runs columns of
+ * 2^13 .. 2^16 points as two passes instead of one cluster launch. */
 int sfntt_ctx_create(int device, sfntt_ctx **out);
 void sfntt_ctx_destroy(sfntt_ctx *ctx);
 const char *sfntt_status_string(int status);
