@@ -130,7 +130,10 @@ int api_ntt_gpu(sfntt_ctx* ctx, int field, int variant, bool inverse, const uint
 
 // Host-memory LDE: columns are processed in chunks on two buffer slots so
 // that the upload of chunk i+1 and the download of chunk i-1 overlap the
-// compute of chunk i.
+// compute of chunk i.  The download (2^added_bits times the upload) is the
+// bottleneck; chunks grow from an eighth of the slot, doubling, so each
+// upload ends before the previous chunk's download and the download stream
+// starts early and stays busy.
 Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out, uint32_t log_n, uint32_t batch,
                     uint32_t added_bits, uint32_t shift_monty, int mode, uint64_t* ns) {
   const uint32_t log_ext = log_n + added_bits;
@@ -138,7 +141,10 @@ Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out
   const size_t per_col = (n + n_ext) * sizeof(uint32_t);
   const size_t target = (size_t)192 << 20;  // bytes per slot
   uint32_t chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(batch, target / per_col));
-  const uint32_t nchunks = (batch + chunk - 1) / chunk;
+  std::vector<uint32_t> starts;  // first column of each chunk
+  for (uint32_t c0 = 0, size = std::max<uint32_t>(1, chunk / 8); c0 < batch; c0 += size, size = std::min(2 * size, chunk))
+    starts.push_back(c0);
+  const uint32_t nchunks = (uint32_t)starts.size();
   SFNTT_TRY(ctx->buf_in.reserve(2 * (size_t)chunk * n * sizeof(uint32_t)));
   SFNTT_TRY(ctx->buf_out.reserve(2 * (size_t)chunk * n_ext * sizeof(uint32_t)));
   uint32_t* din[2] = {ctx->buf_in.as<uint32_t>(), ctx->buf_in.as<uint32_t>() + (size_t)chunk * n};
@@ -165,7 +171,8 @@ Status run_host_lde(sfntt_ctx* ctx, int field, const uint32_t* in, uint32_t* out
   cudaStream_t up = ctx->copy_streams[0], down = ctx->copy_streams[1], comp = ctx->stream;
   for (uint32_t c = 0; c < nchunks && st.ok(); ++c) {
     const int k = c & 1;
-    const uint32_t c0 = c * chunk, cols = std::min(chunk, batch - c0);
+    const uint32_t c0 = starts[c];
+    const uint32_t cols = (c + 1 < nchunks ? starts[c + 1] : batch) - c0;
     auto step = [&]() -> Status {
       if (slot[k].used) {
         SFNTT_CU(cudaStreamWaitEvent(up, slot[k].computed, 0));     // input slot free
