@@ -61,7 +61,7 @@ void check_backend(const sfntt::Context& ctx) {
   sfntt::CudaBackend<F, V> b(ctx);
   constexpr bool bb = F::kField == SFNTT_BABYBEAR;
   const std::string name(b.name());
-  for (uint32_t log_n : {1u, 5u, 10u, 14u}) {
+  for (uint32_t log_n : {1u, 5u, 10u, 14u, 16u}) {  // 14, 16: cluster launches (V4)
     const size_t n = size_t(1) << log_n;
     auto x = lcg(n, 1000 + log_n, bb);
     auto ref = x;
