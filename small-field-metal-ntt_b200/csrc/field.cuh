@@ -153,8 +153,4 @@ __device__ __forceinline__ uint32_t shoup_of(uint32_t w) {
   return (uint32_t)(((uint64_t)w << 32) / F::P);
 }
 
-// The same for M31 without a division: 2^32 / p = 2 + 2 / (2^31 - 1), so for
-// w < p, floor(w 2^32 / p) = 2 w + floor(2 w / p) = 2 w + (w >= 2^30).
-__device__ __forceinline__ uint32_t m31_shoup_of(uint32_t w) { return 2u * w + (w >> 30); }
-
 }  // namespace sfntt

@@ -196,7 +196,9 @@ struct TPass {
   static_assert(!LSTAGE || KD == Kind::S || kRound0Copy, "M31 tile staging starts from the first-round copy");
   static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
   // M31 tile staging: the twiddles of a tile's 2^13 positions, one word each
-  // (the Shoup companion is recomputed, m31_shoup_of), laid out like a
+  // -- the Shoup companion w' = floor(w 2^32 / p), which for the Mersenne
+  // prime (2^32 / p = 2 + 2 / p) is 2w + (w >= 2^30), so w = w' >> 1, one
+  // shift -- laid out like a
   // 2^13-point table with layer L at 8192 - (8192 >> L); layers 0..3 (words
   // [0, 7680)) are ordered by thread: layer j gives thread t its 2^(3-j)
   // twiddles as vectors of v = min(2^(3-j), 4) words at v (g NT + t), group g.
@@ -206,8 +208,8 @@ struct TPass {
       LSTAGE ? (KD == Kind::S ? 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
   static constexpr int kCtasPerSm = (LSTAGE && KD == Kind::S) ? 1 : 2;
 
-  // C = 1, 2 or 4 consecutive staged M31 twiddles from shared memory (p
-  // aligned to C words) into tv[AT, AT + C), with their Shoup companions
+  // C = 1, 2 or 4 consecutive staged M31 twiddles (Shoup companions) from
+  // shared memory (p aligned to C words) into tv[AT, AT + C) as (w, w') pairs
   template <int C, int AT>
   __device__ static __forceinline__ void staged_w(const uint32_t* p, uint2 (&tv)[E / 2]) {
     uint32_t w[4];
@@ -222,7 +224,7 @@ struct TPass {
       w[0] = q.x; w[1] = q.y; w[2] = q.z; w[3] = q.w;
     }
 #pragma unroll
-    for (int i = 0; i < C; ++i) tv[AT + i] = make_uint2(w[i], m31_shoup_of(w[i]));
+    for (int i = 0; i < C; ++i) tv[AT + i] = make_uint2(w[i] >> 1, w[i]);
   }
 
   // ---- twiddles: per-layer base pointer + compile-time offset per slot ----
@@ -534,7 +536,7 @@ struct TPass {
     }
   }
 
-  // M31 per-block twiddles (first words) of the 12 layers over tile positions
+  // M31 per-block twiddles (Shoup companions) of the 12 layers over tile positions
   // [pos_base, pos_base + 2^13): layers 0..3 from the table's first-round
   // copy ([layer][pair group][thread], a pair group = two pairs), layers
   // 4..11 from the table (2^(12-L) consecutive entries each).
@@ -549,13 +551,13 @@ struct TPass {
       const uint32_t t = (rel / v) & (NT - 1u);
       const uint32_t o = (rel / (v * NT)) * v + (rel & (v - 1u));  // the thread's o-th twiddle of layer j
       const uint32_t sp = j == 3u ? off + t : off + 2u * ((o >> 1) * NT + t) + (o & 1u);
-      dst[d] = __ldg(&src0[sp].x);
+      dst[d] = __ldg(&src0[sp].y);
     }
     const uint32_t n = 1u << a.log_n;
     for (uint32_t e = 7680u + tid; e < CTILE_ENTRIES; e += NT) {
       const uint32_t L = 12u - (31u - __clz(8191u - e));  // e in [8192 - 2^(13-L), 8192 - 2^(12-L))
       const uint32_t local = e - (8192u - (8192u >> L));
-      dst[e] = __ldg(&a.tw[(n - (n >> L)) + (pos_base >> (L + 1)) + local].x);
+      dst[e] = __ldg(&a.tw[(n - (n >> L)) + (pos_base >> (L + 1)) + local].y);
     }
   }
 
