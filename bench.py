@@ -66,9 +66,10 @@ def parse():
     ap.add_argument("--slots", type=int, default=8, help="served stream: concurrent request slots")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="served stream: HBM admission budget")
     ap.add_argument("--no-served", action="store_true")
-    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table", "ntt"],
+    ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table", "ntt", "layout"],
                     help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph; "
-                         "ntt: forward + inverse NTT pairs of --batch columns of 2^--log-n points (--field)")
+                         "ntt: forward + inverse NTT pairs of --batch columns of 2^--log-n points (--field); "
+                         "layout: the Merkle-prep permutations of the BabyBear LDE output")
     ap.add_argument("--lanes", type=int, default=8)
     return ap.parse_args()
 
@@ -275,9 +276,10 @@ def main() -> None:
     if a.impl == "reference":
         run_reference(a, rank)
         return
-    if a.workload in ("uneven", "served", "table", "ntt"):
+    if a.workload in ("uneven", "served", "table", "ntt", "layout"):
         if rank == 0:  # single-GPU workloads: under torchrun the other ranks have no work
-            {"uneven": run_uneven, "served": run_served, "table": run_table, "ntt": run_ntt}[a.workload](a)
+            {"uneven": run_uneven, "served": run_served, "table": run_table, "ntt": run_ntt,
+             "layout": run_layout}[a.workload](a)
         return
 
     import torch
@@ -613,6 +615,48 @@ def run_ntt(a) -> None:
             "config": {"workload": f"{a.field} forward + inverse NTT, {cols} column(s) of 2^{log_n} points",
                        "l2": "columns of up to 2^24 words stay resident in L2 (126 MB)"},
             "device": ctx.device_info()}
+    print(json.dumps(line), flush=True)
+
+
+def run_layout(a) -> None:
+    """The Merkle-prep permutations of one BabyBear 2x LDE output (--batch
+    columns of 2^(--log-n + --added-bits) rows): natural row order in place,
+    row-major, row-major in natural order (layout_metrics' first three rows)."""
+    import torch
+    import sfntt
+    torch.cuda.set_device(0)
+    ctx = sfntt.Context(0)
+    n, n_ext = 1 << a.log_n, 1 << (a.log_n + a.added_bits)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234)
+    x = torch.randint(0, BB_P, (a.batch * n,), dtype=torch.int64, device="cuda", generator=gen).to(torch.int32)
+    out = torch.empty(a.batch * n_ext, dtype=torch.int32, device="cuda")
+    rows = torch.empty_like(out)
+    stream = torch.cuda.current_stream().cuda_stream
+    sfntt.CosetLdeBatch(ctx).execute_dev(x.data_ptr(), out.data_ptr(), a.log_n, a.batch, a.added_bits, stream=stream)
+    lb, total = a.log_n + a.added_bits, a.batch * n_ext
+    peak, peak_kind = peaks()
+    res = {}
+    for name, flags, dst in (("natural_in_place", sfntt.LAYOUT_NATURAL, out),
+                             ("row_major", sfntt.LAYOUT_ROW_MAJOR, rows),
+                             ("row_major_natural", sfntt.LAYOUT_ROW_MAJOR | sfntt.LAYOUT_NATURAL, rows)):
+        fn = lambda: sfntt.layout_dev(ctx, out.data_ptr(), dst.data_ptr(), lb, a.batch, flags, stream)
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        res[name] = {"ms": ms, "gbs": 8 * total / (ms * 1e-3) / 1e9, "hbm_frac": 8 * total / (ms * 1e-3) / 1e9 / peak}
+    line = {"metric": f"Merkle-prep layouts of the 2^{lb} x {a.batch} LDE output", "unit": "ms",
+            "value": res["row_major"]["ms"], "higher_is_better": False, "steps": a.steps, "warmup": a.warmup,
+            "layouts": res, "peak_kind": peak_kind, "data": "synthetic",
+            "config": {"workload": f"BabyBear 2x LDE output, {a.batch} columns x 2^{lb} rows, permuted on device",
+                       "algorithmic_bytes": 8 * total}, "device": ctx.device_info()}
     print(json.dumps(line), flush=True)
 
 

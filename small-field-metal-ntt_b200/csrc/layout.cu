@@ -124,25 +124,40 @@ constexpr uint32_t kWideCols = 128;
 
 __global__ void __launch_bounds__(kWideThreads) transpose_wide_kernel(const uint32_t* __restrict__ in,
                                                                       uint32_t* __restrict__ out, uint32_t log_n,
-                                                                      uint32_t batch, uint32_t cblocks,
-                                                                      uint64_t tiles, int bitrev) {
+                                                                      uint32_t batch, uint32_t cblocks, uint32_t tiles,
+                                                                      int bitrev) {
   __shared__ uint32_t tile[kWideCols * 33];
-  const uint64_t n = 1ull << log_n;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-    const uint32_t cb = (uint32_t)(t % cblocks);
-    const uint64_t r0 = (t / cblocks) << 5;
+  // Loads: thread reads tile column warp + 16 q (q < 8) at row lane.  Stores:
+  // thread writes tile row si + 4 q at column sj.  Addresses advance by
+  // shifts from per-tile bases; a bit-reversed row r0 + i (r0 a multiple of
+  // 32, i < 32) is rev(r0) + (rev5(i) << (log n - 5)).
+  const uint32_t si = warp >> 2, sj = ((warp & 3u) << 5) + lane;
+  for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+    const uint32_t rb = t / cblocks, cb = t - rb * cblocks;
     const uint32_t c0 = cb * kWideCols;
+    const uint64_t r0 = (uint64_t)rb << 5;
+    const uint32_t* src = in + ((uint64_t)(c0 + warp) << log_n) + r0 + lane;
 #pragma unroll
-    for (uint32_t j = warp; j < kWideCols; j += kWideThreads / 32)
-      if (c0 + j < batch) tile[j * 33 + lane] = __ldcs(in + (uint64_t)(c0 + j) * n + r0 + lane);
+    for (uint32_t q = 0; q < kWideCols / 16; ++q) {
+      const uint32_t j = warp + 16u * q;
+      if (c0 + j < batch) tile[j * 33 + lane] = __ldcs(src + ((uint64_t)q << (log_n + 4)));
+    }
     __syncthreads();
+    if (c0 + sj < batch) {
+      uint32_t* dst = out + c0 + sj;
+      if (bitrev) {
+        const uint64_t rbase = (uint64_t)rev_bits((uint32_t)r0, log_n) + ((uint64_t)rev_bits(si, 5) << (log_n - 5));
+        dst += rbase * batch;
+        const uint64_t step = (uint64_t)batch << (log_n - 5);  // row rev5(4 q) << (log n - 5) = rev3(q) << (log n - 3)
 #pragma unroll
-    for (uint32_t k = warp; k < 32 * (kWideCols / 32); k += kWideThreads / 32) {
-      const uint32_t i = k / (kWideCols / 32), j = (k % (kWideCols / 32)) * 32 + lane;
-      const uint64_t r = r0 + i;
-      const uint64_t R = bitrev ? rev_bits((uint32_t)r, log_n) : r;
-      if (c0 + j < batch) __stcs(out + R * batch + c0 + j, tile[j * 33 + i]);
+        for (uint32_t q = 0; q < 8; ++q) __stcs(dst + (uint64_t)(rev_bits(4u * q, 5)) * step, tile[sj * 33 + si + 4u * q]);
+      } else {
+        dst += (r0 + si) * batch;
+        const uint64_t step = 4ull * batch;
+#pragma unroll
+        for (uint32_t q = 0; q < 8; ++q) __stcs(dst + q * step, tile[sj * 33 + si + 4u * q]);
+      }
     }
     __syncthreads();
   }
@@ -254,9 +269,10 @@ Status layout_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t lo
   launch_begin(ctx, s);
   if (log_n >= 5 && batch >= kWideCols) {
     const uint32_t cblocks = (batch + kWideCols - 1) / kWideCols;
-    const uint64_t tiles = (uint64_t)cblocks << (log_n - 5);
+    const uint64_t tiles = (uint64_t)cblocks << (log_n - 5);  // batch * n / 4096 at most: < 2^29
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 4));
-    transpose_wide_kernel<<<grid, kWideThreads, 0, s>>>(in, out, log_n, batch, cblocks, tiles, natural ? 1 : 0);
+    transpose_wide_kernel<<<grid, kWideThreads, 0, s>>>(in, out, log_n, batch, cblocks, (uint32_t)tiles,
+                                                        natural ? 1 : 0);
     return launch_check(ctx, natural ? "layout_transpose_bitrev" : "layout_transpose", s, total * 8);
   }
   if (log_n >= 5) {
