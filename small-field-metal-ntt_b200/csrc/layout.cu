@@ -234,7 +234,10 @@ Status bitrev_cols_dev(sfntt_ctx* ctx, const uint32_t* in, uint64_t in_stride, u
   launch_begin(ctx, s);
   if (log_n >= 12) {
     const uint64_t tiles = (uint64_t)batch << (log_n - 12);
-    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 4));
+    // 64 CTAs per SM, two resident: the CTAs in flight hold consecutive tiles,
+    // whose 256-byte runs share DRAM rows (4 per SM, a stride of 4 x SMs
+    // tiles between a CTA's tiles: 0.96 ms for the 2 GiB LDE output; 64: 0.76)
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 64));
     bitrev_cols64_kernel<<<grid, kWideThreads, 0, s>>>(in, in_stride, out, out_stride, log_n, tiles);
     return launch_check(ctx, "layout_bitrev_cols", s, total * 8);
   }
