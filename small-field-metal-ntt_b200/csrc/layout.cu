@@ -273,7 +273,8 @@ Status layout_dev(sfntt_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t lo
   if (log_n >= 5 && batch >= kWideCols) {
     const uint32_t cblocks = (batch + kWideCols - 1) / kWideCols;
     const uint64_t tiles = (uint64_t)cblocks << (log_n - 5);  // batch * n / 4096 at most: < 2^29
-    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 4));
+    // 64 CTAs per SM, as the bit reversal (row-major 0.83 -> 0.80 ms on the 2 GiB LDE output)
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)ctx->sm_count * 64));
     transpose_wide_kernel<<<grid, kWideThreads, 0, s>>>(in, out, log_n, batch, cblocks, (uint32_t)tiles,
                                                         natural ? 1 : 0);
     return launch_check(ctx, natural ? "layout_transpose_bitrev" : "layout_transpose", s, total * 8);
