@@ -86,3 +86,33 @@ def test_single_ntt_entry_points_use_the_cluster(ctx):
     out, names = _kernels(ctx, lambda: b.inverse_ntt_gpu(prod, log_n)[0])
     assert any("_inv_cluster" in k for k in names), names
     assert [O.bb_from_monty(int(v)) for v in out[:4]] == [3, 10, 8, 0] and not out[4:].any()
+
+
+def test_no_cluster_switch_keeps_the_passes(tmp_path):
+    """SFNTT_NO_CLUSTER=1 (read at context creation) runs 2^13..2^16-point
+    columns as two passes: same results, no cluster kernel."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    script = tmp_path / "no_cluster.py"
+    script.write_text(
+        "import sys\n"
+        f"sys.path[:0] = [{str(root)!r}, {str(root / 'small-field-metal-ntt_b200')!r}]\n"
+        "import numpy as np, sfntt\n"
+        "from oracle import oracle as O\n"
+        "ctx = sfntt.Context(0)\n"
+        "b = sfntt.CudaCtGsR4(ctx)\n"
+        "x = O.lcg(3 << 15, 5, O.M31_P)\n"
+        "ctx.kernel_timing(True)\n"
+        "fw = b.forward_ntt_batch_gpu(x, 15, 3)[0]\n"
+        "names = set(ctx.kernel_times())\n"
+        "assert not any('cluster' in k for k in names), names\n"
+        "n = 1 << 15\n"
+        "assert all(np.array_equal(fw[c * n:(c + 1) * n], O.m31_forward(x[c * n:(c + 1) * n])) for c in range(3))\n"
+        "assert np.array_equal(b.inverse_ntt_batch_gpu(fw, 15, 3)[0], x)\n"
+        "print('ok')\n")
+    env = dict(os.environ, SFNTT_NO_CLUSTER="1")
+    r = subprocess.run([sys.executable, str(script)], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
