@@ -348,3 +348,21 @@ def test_extension_size_cannot_wrap(ctx):
     items = [{"field": BB, "log_n": 5, "batch": 1, "added_bits": huge, "d_in": d.data_ptr(), "d_out": d.data_ptr()}]
     with pytest.raises(sfntt.InvalidSize):
         sfntt.LdeBatch(ctx, items).prepare()
+
+
+@pytest.mark.parametrize("log_n,batch,added", [(21, 2, 1), (22, 1, 1), (21, 1, 2)])
+def test_large_lde_multi_pass_layers(ctx, log_n, batch, added):
+    """Above 2^20 rows the LDE's outer layer ranges split into contiguous and
+    strided passes (BabyBear and M31), and the natural-order form takes the
+    bit-reversal route: every column against the oracle."""
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    x = O.lcg(batch << log_n, 60 + log_n, O.BB_P, monty=True)
+    r = sfntt.CosetLdeBatch(ctx).execute(x, log_n, batch, added)
+    assert np.array_equal(r.data, O.bb_coset_lde(x, log_n, batch, added, threads=8))
+    m = O.lcg(batch << log_n, 70 + log_n, O.M31_P)
+    assert np.array_equal(sfntt.M31Lde(ctx).execute(m, log_n, batch, added).data,
+                          O.m31_lde(m, log_n, batch, added, threads=8))
+    if batch == 1 and added == 1:
+        rev = lambda bits: np.array([int(format(k, f"0{bits}b")[::-1], 2) for k in range(1 << bits)])
+        nat = sfntt.CosetLdeBatch(ctx, natural=True).execute(x[rev(log_n)], log_n, 1, added).data
+        assert np.array_equal(nat, r.data[rev(log_n + added)])
