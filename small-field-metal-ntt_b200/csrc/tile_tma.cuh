@@ -154,14 +154,19 @@ struct TPass {
         g.c1 = (int32_t)(r << (CB - 5));
         g.c2 = (int32_t)(t - r * a.batch);
       } else {
-        const uint32_t per_chunk = a.batch << (a.log_n - a.lo - P);
-        const uint32_t lchunk = t / per_chunk;
-        const uint32_t r = t - lchunk * per_chunk;
-        g.hb = r / a.batch;
+        // chunk pairs {2p, 2p+1} slowest, then high block and column, the
+        // pair's two chunks alternating: consecutive tiles read neighbouring
+        // 128-byte runs of the same rows
+        const uint32_t per_pair = (a.batch << (a.log_n - a.lo - P)) << 1;
+        const uint32_t pair = t / per_pair;
+        const uint32_t r = t - pair * per_pair;
+        const uint32_t rest = r >> 1;
+        const uint32_t lchunk = 2u * pair + (r & 1u);
+        g.hb = rest / a.batch;
         g.pos_base = lchunk << 5;
         g.s1 = (int32_t)lchunk;
         g.s3 = (int32_t)g.hb;
-        g.s4 = (int32_t)(r - g.hb * a.batch);
+        g.s4 = (int32_t)(rest - g.hb * a.batch);
       }
       return g;
     }
@@ -205,7 +210,7 @@ struct TPass {
   static constexpr uint32_t CTILE_ENTRIES = 8190u;
   // staged twiddle bytes in shared memory, CTAs per SM
   static constexpr uint32_t SMEM_TW_BYTES =
-      LSTAGE ? (KD == Kind::S ? 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
+      LSTAGE ? (KD == Kind::S ? 2u * 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
   static constexpr int kCtasPerSm = (LSTAGE && KD == Kind::S) ? 1 : 2;
 
   // C = 1, 2 or 4 consecutive staged M31 twiddles (Shoup companions) from
@@ -611,10 +616,14 @@ struct TPass {
         // Every thread passed the previous tile's pre-store barrier after its
         // last twiddle read; the barrier here publishes the new copy (the
         // positions are a function of t, the same for the whole CTA).
-        const uint32_t key = (KD == Kind::C) ? g.pos_base : (uint32_t)g.s1;
+        const uint32_t key = (KD == Kind::C) ? g.pos_base : ((uint32_t)g.s1 >> 1);
         if (key != staged) {
-          if constexpr (KD == Kind::C) stage_ctile(reinterpret_cast<uint32_t*>(tws), a, g.pos_base, tid);
-          else stage_lchunk(tws, a.tw, a.lo, (uint32_t)g.s1, tid);
+          if constexpr (KD == Kind::C) {
+            stage_ctile(reinterpret_cast<uint32_t*>(tws), a, g.pos_base, tid);
+          } else {  // both chunks of the pair
+            stage_lchunk(tws, a.tw, a.lo, 2u * key, tid);
+            stage_lchunk(tws + LCHUNK_ENTRIES, a.tw, a.lo, 2u * key + 1u, tid);
+          }
           staged = key;
           __syncthreads();
         }
@@ -626,7 +635,10 @@ struct TPass {
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
       ld<kFirst>(cur, v, tid);
       if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
-      rounds<0>(cur, v, a, tws, g, tid);
+      if constexpr (LSTAGE && KD == Kind::S)
+        rounds<0>(cur, v, a, tws + ((uint32_t)g.s1 & 1u) * LCHUNK_ENTRIES, g, tid);
+      else
+        rounds<0>(cur, v, a, tws, g, tid);
       finish(v, a, g, tid);
       st<kLast>(cur, v, tid);
       tma::fence_proxy_async();
