@@ -7,6 +7,8 @@ import subprocess
 import sys
 from pathlib import Path
 
+import pytest
+
 ROOT = Path(__file__).resolve().parents[1]
 
 
@@ -37,3 +39,23 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["e2e"]["value"] == d["value"]
     assert "workload" in d["config"]
+
+
+@pytest.mark.gpu
+def test_gpu_arm_prints_one_contract_line():
+    r = _bench("--log-n", "14", "--batch", "16", "--steps", "3", "--warmup", "3", "--no-secondary", "--no-served",
+               "--cpu-seconds", "1", "--e2e-steps", "2", timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = [l for l in r.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1, lines
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "roofline", "cpu_baseline", "e2e",
+              "gpu_launches", "clocks"):
+        assert k in d, k
+    assert d["n_gpus"] == 1 and d["steps"] == 3 and d["warmup"] == 3 and d["value"] > 0
+    assert d["gpu_launches"] > 0
+    assert {"bound", "achieved", "peak", "unit", "frac", "traffic"} <= set(d["roofline"])
+    assert {"value", "unit", "cores", "kind", "sample"} <= set(d["cpu_baseline"])
+    assert d["e2e"]["h2d_bytes_per_step"] == 16 << 16 and d["e2e"]["d2h_bytes_per_step"] == 2 * (16 << 16)
+    assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
