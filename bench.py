@@ -35,7 +35,7 @@ sys.path.insert(0, str(ROOT))
 BB_P = 2013265921
 KB_P = 2130706433  # KoalaBear, 2^31 - 2^24 + 1
 METRIC = "BabyBear coset LDE 2^20x256 2x"
-PUBLISHED_MS = 821.0  # BASELINE.md / README.md:58 (Apple M3, Metal)
+PUBLISHED_MS = 821.0  # the reference's README.md:58 (Apple M3, Metal)
 
 
 def parse():
@@ -64,8 +64,10 @@ def parse():
     ap.add_argument("--rates", default="50,100,200,500,1000,2000", help="served stream: arrival rates, req/s")
     ap.add_argument("--requests", type=int, default=120, help="served stream: requests per rate")
     ap.add_argument("--slots", type=int, default=8, help="served stream: concurrent request slots")
+    ap.add_argument("--pack", type=int, default=32, help="served stream: most same-shape requests per launch")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="served stream: HBM admission budget")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch comparison in the LDE line")
     ap.add_argument("--workload", default="lde", choices=["lde", "uneven", "served", "table", "ntt", "layout"],
                     help="lde: the headline LDE (default); uneven: 64 mixed polynomials, plain loop vs one graph; "
                          "ntt: forward + inverse NTT pairs of --batch columns of 2^--log-n points (--field); "
@@ -261,7 +263,8 @@ def run_reference(a, rank: int) -> None:
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": ms / PUBLISHED_MS if metric_name(a) == METRIC else None,
             "dtype": dtype_of(a), "data": "synthetic",
-            "config": workload(a),
+            "config": {**workload(a), "parallelism": f"replicas x{a.gpus}" if a.gpus > 1 else "single GPU"},
+            "step_stats": step_stats([t * 1e3 for t in times]),
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -334,15 +337,19 @@ def main() -> None:
     launches0 = ctx.launch_count()
     barrier()
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # one event per step boundary on the launching stream: the total and the
+    # per-step spread come from the same timed run
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps + 1)]
     w0 = time.time()
-    ev0.record()
-    for _ in range(a.steps):
+    evs[0].record()
+    for i in range(a.steps):
         step()
-    ev1.record()
+        evs[i + 1].record()
     torch.cuda.synchronize()
     w1 = time.time()
     barrier()
+    ev0, ev1 = evs[0], evs[-1]
+    per_step = [evs[i].elapsed_time(evs[i + 1]) for i in range(a.steps)]
     launches = ctx.launch_count() - launches0
     clocks = sampler.stop(w0, w1)
     # per-kernel breakdown on a separate run: events around every launch
@@ -410,6 +417,7 @@ def main() -> None:
     del x, out
     torch.cuda.empty_cache()
     served = None if (a.no_served or world > 1) else served_sweep(a, ctx, sfntt, torch)
+    uneven = None if (a.no_uneven or world > 1 or m31) else uneven_metrics(a, ctx, sfntt, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -420,6 +428,7 @@ def main() -> None:
         return
     line = {"metric": metric_name(a), "value": value, "unit": "ms", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "step_stats": step_stats(per_step),
             "vs_baseline": value / PUBLISHED_MS if metric_name(a) == METRIC else None,
             "dtype": dtype_of(a)[:-1] + ", exact)",
             "data": "synthetic: seeded uniform canonical values in [0, p)" + ("" if m31 else ", Montgomery on device"),
@@ -430,7 +439,48 @@ def main() -> None:
             "roofline": roofline, "int_roofline": int_roofline, "kernels": kernels, "clocks": clocks, "e2e": e2e,
             "cpu_baseline": cpu,
             "secondary": secondary, "layout": layouts, "served": served, "device": ctx.device_info()}
+    line.update(headline_keys(secondary, uneven, served))
+    if uneven is not None:
+        line["uneven"] = uneven
     print(json.dumps(line), flush=True)
+
+
+def step_stats(ms: list) -> dict:
+    """Spread of the per-step device times (the reference's bench reports
+    median, min, max, stddev, p95 and CV: benches/ntt_benchmark.rs:63-120)."""
+    import numpy as np
+    v = np.asarray(ms, dtype=float)
+    mean = float(v.mean())
+    sd = float(v.std(ddof=1)) if v.size > 1 else 0.0
+    return {"mean_ms": mean, "median_ms": float(np.median(v)), "min_ms": float(v.min()), "max_ms": float(v.max()),
+            "p95_ms": float(np.percentile(v, 95)), "stddev_ms": sd, "cv_pct": 100.0 * sd / mean if mean else 0.0,
+            "n": int(v.size)}
+
+
+def headline_keys(secondary, uneven, served) -> dict:
+    """The other configurations' headline numbers as top-level scalars:
+    the M31 2^16 forward + inverse pair, the BabyBear 2^20 and 2^24 pairs, the
+    uneven batch (plain loop and one launch) and the served stream at its
+    highest rate."""
+    out = {}
+    if secondary:
+        out["m31_2^16_fwd_inv_us"] = secondary["m31"]["16"]["fwd_inv_us"]
+        for k in ("10", "16", "20", "24"):
+            out[f"bb_2^{k}_fwd_inv_us"] = secondary["bb"][k]["fwd_inv_us"]
+        out["bb_2^24_gelem_s"] = secondary["bb"]["24"]["gelem_s"]
+    if uneven:
+        for k in ("plain_loop_ms", "graph_ms", "persistent_ms", "speedup", "persistent_speedup"):
+            if k in uneven:
+                out[f"uneven_{k}"] = uneven[k]
+    if served:
+        for prefix, top in (("served", served["at_max_rate"]), ("served_small", served["small"]["at_max_rate"])):
+            out[f"{prefix}_rate_req_s"] = top["rate"]
+            out[f"{prefix}_melem_s"] = top["served_melem_s"]
+            out[f"{prefix}_plain_melem_s"] = top["plain_melem_s"]
+            out[f"{prefix}_throughput_ratio"] = top["throughput_ratio"]
+            out[f"{prefix}_p99_ms"] = top["served_p99_ms"]
+            out[f"{prefix}_plain_p99_ms"] = top["plain_p99_ms"]
+    return out
 
 
 def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
@@ -489,18 +539,65 @@ def layout_metrics(a, ctx, sfntt, torch, x, out, stream) -> dict:
     return res
 
 
+SMALL_STREAM = {"log_n_weights": {14: 1, 15: 1, 16: 1}, "cols_range": (8, 32),
+                "rates": (1000.0, 5000.0, 20000.0, 100000.0)}
+
+
+def _trace_stats(lat, mk, elems_out, bytes_alg, peak, launches=None) -> dict:
+    import numpy as np
+    d = {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+         "mean_ms": float(lat.mean() * 1e3), "makespan_s": mk,
+         "melem_per_s": elems_out / mk / 1e6, "hbm_frac": bytes_alg / mk / (peak * 1e9)}
+    if launches is not None:
+        d["launches"] = launches
+    return d
+
+
+def _replay_stream(a, ctx, sfntt, reqs, unit_arrivals, rates, budget, peak, host=None, dropin=None) -> list:
+    """One stream at each rate: the plain sequential per-request loop (one
+    slot, one launch per request), continuous batching (--slots slots, one
+    launch per request) and continuous batching with packing (up to --pack
+    same-shape requests per launch); `dropin` (optional) replays the
+    drop-in per-request host call."""
+    elems_out = sum(it["batch"] << (it["log_n"] + it["added_bits"]) for it in reqs)
+    bytes_alg = sum(4 * (it["batch"] << it["log_n"]) * (1 + (1 << it["added_bits"])) for it in reqs)
+    out = []
+    for rate in rates:
+        arr = unit_arrivals / rate
+        row = {"rate_req_s": rate}
+        for name, slots, pack in (("plain", 1, 1), ("served", a.slots, 1), ("packed", a.slots, a.pack)):
+            st = {}
+            lat, mk = sfntt.serve_trace(ctx, reqs, arr, slots=slots, budget_bytes=budget, host=host, max_pack=pack,
+                                        stats=st)
+            row[name] = _trace_stats(lat, mk, elems_out, bytes_alg, peak, st.get("launches"))
+        if dropin is not None:
+            lat, mk = dropin(arr)
+            row["dropin_host_call"] = _trace_stats(lat, mk, elems_out, bytes_alg, peak, len(reqs))
+        for name in ("served", "packed"):
+            row[f"{name}_throughput_ratio"] = row[name]["melem_per_s"] / row["plain"]["melem_per_s"]
+            row[f"{name}_p99_ratio"] = row[name]["p99_ms"] / row["plain"]["p99_ms"]
+        row["throughput_ratio"] = row["packed_throughput_ratio"]
+        row["p99_ratio"] = row["packed_p99_ratio"]
+        out.append(row)
+    return out
+
+
 def served_sweep(a, ctx, sfntt, torch) -> dict:
-    """The served stream: Poisson arrivals of LDE requests at each rate in
-    --rates; field 50/50 M31 / BabyBear, log n 14..22 weighted toward 18-20,
-    8..256 columns, blow-up 2 or 4, seeded; inputs are seeded slices of one
-    resident 4 GiB pool of uniform values in [0, p); HBM admission budget
-    --budget-gb; twiddle tables resident.  Each rate replays the same trace
-    through the plain sequential per-request loop (one slot) and through the
-    continuously batching server (--slots slots); latency = completion seen by
-    the host - arrival."""
+    """The served streams, each replayed at several Poisson arrival rates
+    through the plain sequential per-request loop, continuous batching and
+    continuous batching with packing (same arena, kernels and resident tables):
+      mixed -- the configured stream: field 50/50 M31 / BabyBear, log n 14..22
+               weighted toward 18-20, 8..256 columns, blow-up 2 or 4, seeded;
+               inputs are seeded slices of one resident 4 GiB pool;
+      small -- requests that leave most of the GPU idle (log n 14..16, 8..32
+               columns), host requests (input copied in, output copied back),
+               plus the drop-in per-request host call replayed in order.
+    HBM admission budget --budget-gb; latency = completion seen by the host -
+    arrival."""
     import numpy as np
     rates = [float(r) for r in a.rates.split(",") if r]
     budget = int(a.budget_gb * (1 << 30))
+    peak, _ = peaks()
     pool_words = 1 << 30
     gen = torch.Generator(device="cuda")
     gen.manual_seed(4242)
@@ -511,39 +608,68 @@ def served_sweep(a, ctx, sfntt, torch) -> dict:
         need = it["batch"] << it["log_n"]
         off = int(rng.integers(0, (pool_words - need) // 64 + 1)) * 64
         it["d_in"] = pool.data_ptr() + 4 * off
-    elems_out = sum(it["batch"] << (it["log_n"] + it["added_bits"]) for it in reqs)
-    bytes_alg = sum(4 * (it["batch"] << it["log_n"]) * (1 + (1 << it["added_bits"])) for it in reqs)
     # warm-up: tables, the arena and every kernel shape once
-    sfntt.serve_trace(ctx, reqs, np.zeros(len(reqs)), slots=a.slots, budget_bytes=budget)
+    sfntt.serve_trace(ctx, reqs, np.zeros(len(reqs)), slots=a.slots, budget_bytes=budget, max_pack=a.pack)
     launches0 = ctx.launch_count()
-    peak, _ = peaks()
-    out = []
-    for rate in rates:
-        arr = unit_arrivals / rate
-        row = {"rate_req_s": rate}
-        for name, slots in (("plain", 1), ("served", a.slots)):
-            lat, mk = sfntt.serve_trace(ctx, reqs, arr, slots=slots, budget_bytes=budget)
-            row[name] = {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                         "mean_ms": float(lat.mean() * 1e3), "makespan_s": mk,
-                         "melem_per_s": elems_out / mk / 1e6, "hbm_frac": bytes_alg / mk / (peak * 1e9)}
-        row["throughput_ratio"] = row["served"]["melem_per_s"] / row["plain"]["melem_per_s"]
-        row["p99_ratio"] = row["served"]["p99_ms"] / row["plain"]["p99_ms"]
-        out.append(row)
+    mixed = _replay_stream(a, ctx, sfntt, reqs, unit_arrivals, rates, budget, peak)
     launches = ctx.launch_count() - launches0
     del pool
     torch.cuda.empty_cache()
-    top = max(out, key=lambda r: r["rate_req_s"])
+
+    # the small-request stream, host requests
+    sreqs, s_unit = sfntt.served_workload(a.requests, rate=1.0, seed=2026,
+                                          cols_range=SMALL_STREAM["cols_range"],
+                                          log_n_weights=SMALL_STREAM["log_n_weights"])
+    host = []
+    for i, it in enumerate(sreqs):
+        p = BB_P if it["field"] == sfntt.FIELD_BABYBEAR else 2147483647
+        x = ctx.pinned(it["batch"] << it["log_n"])
+        x.array[:] = np.random.default_rng(500 + i).integers(0, p, x.array.size, dtype=np.uint32)
+        if it["field"] == sfntt.FIELD_BABYBEAR:
+            x.array[:] = ((x.array.astype(np.uint64) << 32) % BB_P).astype(np.uint32)  # Montgomery form
+        y = ctx.pinned(it["batch"] << (it["log_n"] + it["added_bits"]))
+        host.append((x, y))
+    host_arrays = [(x.array, y.array) for x, y in host]
+    ldes = {sfntt.FIELD_BABYBEAR: sfntt.CosetLdeBatch(ctx), sfntt.FIELD_M31: sfntt.M31Lde(ctx)}
+
+    def dropin(arr):
+        """The drop-in call per request (sfntt_coset_lde / sfntt_m31_lde, host
+        buffers, synchronous), one after another as they arrive."""
+        lat = np.zeros(len(sreqs))
+        t0 = time.perf_counter()
+        for i, it in enumerate(sreqs):
+            while time.perf_counter() - t0 < arr[i]:
+                pass
+            ldes[it["field"]].execute(host_arrays[i][0], it["log_n"], it["batch"], it["added_bits"],
+                                      out=host_arrays[i][1])
+            lat[i] = time.perf_counter() - t0 - arr[i]
+        return lat, time.perf_counter() - t0
+
+    dropin(np.zeros(len(sreqs)))  # warm-up: tables and staging buffers
+    sfntt.serve_trace(ctx, sreqs, np.zeros(len(sreqs)), slots=a.slots, budget_bytes=budget, host=host_arrays,
+                      max_pack=a.pack)
+    small = _replay_stream(a, ctx, sfntt, sreqs, s_unit, SMALL_STREAM["rates"], budget, peak, host=host_arrays,
+                           dropin=dropin)
+    for x, y in host:
+        x.free()
+        y.free()
+
+    def summary(rows):
+        top = max(rows, key=lambda r: r["rate_req_s"])
+        return {"rate": top["rate_req_s"], "plain_p50_ms": top["plain"]["p50_ms"],
+                "plain_p99_ms": top["plain"]["p99_ms"], "served_p50_ms": top["packed"]["p50_ms"],
+                "served_p99_ms": top["packed"]["p99_ms"], "plain_melem_s": top["plain"]["melem_per_s"],
+                "served_melem_s": top["packed"]["melem_per_s"], "throughput_ratio": top["packed_throughput_ratio"],
+                "unpacked_throughput_ratio": top["served_throughput_ratio"]}
+
     return {"workload": f"{a.requests} requests per rate, Poisson arrivals, field 50/50, log n 14..22 weighted "
                         f"18-20, columns U[8,256], blow-up 2/4, seed 2025; inputs: slices of a resident 4 GiB pool",
-            "slots": a.slots, "budget_gb": a.budget_gb, "requests": a.requests,
-            "output_gelem_per_trace": elems_out / 1e9, "algorithmic_gb_per_trace": bytes_alg / 1e9,
+            "slots": a.slots, "max_pack": a.pack, "budget_gb": a.budget_gb, "requests": a.requests,
             "gpu_launches": launches,
-            "at_max_rate": {"rate": top["rate_req_s"], "plain_p50_ms": top["plain"]["p50_ms"],
-                            "plain_p99_ms": top["plain"]["p99_ms"], "served_p50_ms": top["served"]["p50_ms"],
-                            "served_p99_ms": top["served"]["p99_ms"], "plain_melem_s": top["plain"]["melem_per_s"],
-                            "served_melem_s": top["served"]["melem_per_s"],
-                            "throughput_ratio": top["throughput_ratio"]},
-            "sweep": out}
+            "at_max_rate": summary(mixed), "sweep": mixed,
+            "small": {"workload": f"{a.requests} requests per rate, field 50/50, log n 14..16, columns U[8,32], "
+                                  "blow-up 2/4, seed 2026; host requests (pinned input copied in, output copied back)",
+                      "at_max_rate": summary(small), "sweep": small}}
 
 
 def run_served(a) -> None:

@@ -3,7 +3,7 @@
  *
  * Drop-in boundary for the NTT hot path of moven0831/small-field-metal-ntt.
  * The reference is a Rust crate; a Rust FFI crate (sfntt-sys) binds these
- * symbols one to one (see INTEGRATION.md).  All functions are plain C:
+ * symbols one to one.  All functions are plain C:
  * pointers, sizes and integer status codes, no C++ or torch types.
  *
  * Conventions (same as the reference):
@@ -234,7 +234,13 @@ typedef enum sfntt_plan {
     SFNTT_PLAN_AUTO = 0,           /* tuned plan for the item's key, else the context default */
     SFNTT_PLAN_TMA = 1,            /* persistent TMA engine, per-position strided twiddles */
     SFNTT_PLAN_TMA_FOUR_STEP = 2,  /* persistent TMA engine, four-step strided passes */
-    SFNTT_PLAN_TILE = 3            /* first (non-TMA) shared-memory tile engine */
+    SFNTT_PLAN_TILE = 3,           /* first (non-TMA) shared-memory tile engine */
+    SFNTT_PLAN_ENGINE_MASK = 3,
+    /* flags on the TMA engines: */
+    SFNTT_PLAN_SPLIT12 = 4,        /* layer ranges above 12 layers: a 12-layer contiguous pass, the rest
+                                      in strided passes (default: 8-layer strided passes, the rest
+                                      contiguous) -- the stages per pass */
+    SFNTT_PLAN_ONE_CTA = 8         /* one persistent CTA per SM (default: as many as fit) */
 } sfntt_plan;
 
 typedef struct sfntt_lde_item {
@@ -261,7 +267,10 @@ uint64_t sfntt_graph_kernel_count(const sfntt_graph *graph);
 void sfntt_graph_destroy(sfntt_graph *graph);
 /* Autotuner: for each distinct key (field, log_n, columns rounded up to a power
  * of two, added_bits) time every plan `reps` times on the first item with that
- * key and keep the fastest for SFNTT_PLAN_AUTO items.  The table is text. */
+ * key and keep the fastest for SFNTT_PLAN_AUTO items: the engine (TMA with
+ * per-position or four-step strided twiddles, or the non-TMA tile engine),
+ * the layer split (SFNTT_PLAN_SPLIT12, where a range exceeds 12 layers) and
+ * the CTAs per SM (SFNTT_PLAN_ONE_CTA).  The table is text. */
 int sfntt_autotune(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int reps);
 int sfntt_tune_save(sfntt_ctx *ctx, const char *path);
 int sfntt_tune_load(sfntt_ctx *ctx, const char *path);
@@ -299,6 +308,19 @@ int sfntt_server_result(sfntt_server *server, uint64_t ticket, uint32_t **d_out)
 int sfntt_server_release(sfntt_server *server, uint64_t ticket);
 /* Requests queued or running. */
 size_t sfntt_server_pending(const sfntt_server *server);
+/* Packing (no reference counterpart; the reference encodes many columns of
+ * one LDE into one command buffer, src/ntt/babybear/metal_ct_gs_r4.rs:181-246,
+ * and this applies it across requests): when the request at the front of the
+ * queue launches, up to max_requests - 1 queued requests of the same field,
+ * log_n, added_bits, shift and plan that each leave part of the GPU idle join
+ * it as further columns of one batch, as long as the launch fits the GPU's
+ * free width.  Their inputs are gathered into one arena block (device
+ * requests: a device-to-device copy from d_in), one LDE runs over all the
+ * columns, and each request's output is its slice of the launch's output.
+ * max_requests = 1 (the default) launches every request alone. */
+int sfntt_server_set_packing(sfntt_server *server, int max_requests);
+/* Launches (alone or packed) the server has admitted. */
+uint64_t sfntt_server_launches(const sfntt_server *server);
 /* Replay a request trace against the wall clock: request i is submitted
  * arrival_s[i] seconds (sorted) after the start, finished requests are
  * released at once; latency_s[i] = completion seen by the host - arrival.
@@ -308,6 +330,12 @@ size_t sfntt_server_pending(const sfntt_server *server);
 int sfntt_serve_trace(sfntt_ctx *ctx, const sfntt_lde_item *reqs, const uint32_t *const *h_in,
                       uint32_t *const *h_out, const double *arrival_s, size_t count, int slots,
                       size_t budget_bytes, double *latency_s, double *makespan_s);
+/* The same with packing (max_pack requests per launch, 1 = none); *launches
+ * (optional) receives the number of launches the trace took. */
+int sfntt_serve_trace_packed(sfntt_ctx *ctx, const sfntt_lde_item *reqs, const uint32_t *const *h_in,
+                             uint32_t *const *h_out, const double *arrival_s, size_t count, int slots,
+                             int max_pack, size_t budget_bytes, double *latency_s, double *makespan_s,
+                             uint64_t *launches);
 
 /* Allocation-free NTT (no counterpart in the reference).  For callers that
  * cannot allocate device memory when they run a transform (a fixed memory
@@ -319,8 +347,10 @@ int sfntt_serve_trace(sfntt_ctx *ctx, const sfntt_lde_item *reqs, const uint32_t
  * 2^20 (else SFNTT_INVALID_SIZE); the twiddles for (field, log_n) must be
  * resident (sfntt_prepare; else SFNTT_INVALID_ARGUMENT).  The first call on a
  * device resolves the array's address (cudaGetSymbolAddress): make it before
- * any stream capture.  All calls share the array; calls that overlap on the
- * GPU race on it. */
+ * any stream capture.  The address is cached per device until the process
+ * exits, so resetting a device (cudaDeviceReset) while the library is loaded
+ * is not supported by this call.  All calls share the array; calls that
+ * overlap on the GPU race on it. */
 int sfntt_stockham_noalloc(sfntt_ctx *ctx, int field, int inverse, uint32_t *d_data, uint32_t log_n,
                            uint32_t batch, void *stream);
 

@@ -39,16 +39,30 @@ namespace sfntt {
 namespace {
 
 struct Knobs {
-  bool no_tma, ntt_plain, lde_plain;
+  bool no_tma, ntt_plain, lde_plain, split_c12;
+  int tma_ctas;
 };
 
+// A plan is an engine (SFNTT_PLAN_TMA / _TMA_FOUR_STEP / _TILE) plus optional
+// flags: SFNTT_PLAN_SPLIT12 (layer ranges above 12 layers: a 12-layer
+// contiguous pass, the rest in strided passes) and SFNTT_PLAN_ONE_CTA (one
+// persistent CTA per SM instead of the kernel's full residency).
 Knobs plan_knobs(int plan, const sfntt_ctx* ctx) {
-  switch (plan) {
-    case SFNTT_PLAN_TMA: return {false, true, false};
-    case SFNTT_PLAN_TMA_FOUR_STEP: return {false, true, true};
-    case SFNTT_PLAN_TILE: return {true, false, false};
-    default: return {ctx->no_tma, ctx->ntt_plain, ctx->lde_plain};
+  const bool split = (plan & SFNTT_PLAN_SPLIT12) != 0;
+  const int ctas = (plan & SFNTT_PLAN_ONE_CTA) ? 1 : 0;
+  switch (plan & SFNTT_PLAN_ENGINE_MASK) {
+    case SFNTT_PLAN_TMA: return {false, true, false, split, ctas};
+    case SFNTT_PLAN_TMA_FOUR_STEP: return {false, true, true, split, ctas};
+    case SFNTT_PLAN_TILE: return {true, false, false, false, 0};
+    default: return {ctx->no_tma, ctx->ntt_plain, ctx->lde_plain, ctx->split_c12, ctx->tma_ctas};
   }
+}
+
+bool valid_plan(int plan) {
+  if (plan & ~(SFNTT_PLAN_ENGINE_MASK | SFNTT_PLAN_SPLIT12 | SFNTT_PLAN_ONE_CTA)) return false;
+  const int e = plan & SFNTT_PLAN_ENGINE_MASK;
+  if (e == SFNTT_PLAN_AUTO) return plan == SFNTT_PLAN_AUTO;
+  return e != SFNTT_PLAN_TILE || plan == SFNTT_PLAN_TILE;
 }
 
 uint32_t pow2_ceil(uint32_t x) {
@@ -82,11 +96,14 @@ Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
     auto f = ctx->tuned.find(key_of(it));
     plan = f == ctx->tuned.end() ? SFNTT_PLAN_AUTO : f->second;
   }
-  const Knobs saved{ctx->no_tma, ctx->ntt_plain, ctx->lde_plain};
+  if (!valid_plan(plan)) return {SFNTT_INVALID_ARGUMENT, "item: unknown plan " + std::to_string(plan)};
+  const Knobs saved{ctx->no_tma, ctx->ntt_plain, ctx->lde_plain, ctx->split_c12, ctx->tma_ctas};
   const Knobs k = plan_knobs(plan, ctx);
   ctx->no_tma = k.no_tma;
   ctx->ntt_plain = k.ntt_plain;
   ctx->lde_plain = k.lde_plain;
+  ctx->split_c12 = k.split_c12;
+  ctx->tma_ctas = k.tma_ctas;
   Status st = is_monty(it.field)
                   ? monty_lde_dev(ctx, it.field, it.d_in, it.d_out, it.log_n, it.batch, it.added_bits,
                                   it.shift_monty, SFNTT_LDE_FUSED, s)
@@ -94,6 +111,8 @@ Status run_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
   ctx->no_tma = saved.no_tma;
   ctx->ntt_plain = saved.ntt_plain;
   ctx->lde_plain = saved.lde_plain;
+  ctx->split_c12 = saved.split_c12;
+  ctx->tma_ctas = saved.tma_ctas;
   return st;
 }
 
@@ -114,13 +133,17 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
       SFNTT_TRY(monty_twist_table(ctx, f, it.log_n - 8, 8, false, s, &t));
     }
     // strided-pass twists of the four-step plain-NTT plans inside [0, log_n - 8)
+    // (both layer splits: a graph captured later may use either)
     for (uint32_t top : {it.log_n, ext}) {
       const uint32_t lo = top >= 13 ? top - 8 : 0;
       if (lo > 12) {
-        const uint32_t s_cnt = (lo - 12 + 7) / 8, c = lo - 8 * s_cnt;
-        for (uint32_t i = 0; i < s_cnt; ++i) {
-          SFNTT_TRY(monty_twist_table(ctx, f, c + 8 * i, 8, true, s, &t));
-          SFNTT_TRY(monty_twist_table(ctx, f, c + 8 * i, 8, false, s, &t));
+        for (bool c12 : {false, true}) {
+          uint32_t plo[4], pcnt[4];
+          const int k = tma_split(0, lo, plo, pcnt, c12);
+          for (int i = 1; i < k; ++i) {
+            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], true, s, &t));
+            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], false, s, &t));
+          }
         }
       }
     }
@@ -295,9 +318,17 @@ int sfntt_autotune(sfntt_ctx* ctx, const sfntt_lde_item* items, size_t count, in
       SFNTT_TRY(sfntt::prepare_item(ctx, it, s));
       float best_ms = 1e30f;
       int best = SFNTT_PLAN_TMA;
-      const int plans[] = {SFNTT_PLAN_TMA, SFNTT_PLAN_TMA_FOUR_STEP, SFNTT_PLAN_TILE};
+      std::vector<int> plans;
+      for (int e : {(int)SFNTT_PLAN_TMA, (int)SFNTT_PLAN_TMA_FOUR_STEP}) {
+        if (it.field == SFNTT_M31 && e == SFNTT_PLAN_TMA_FOUR_STEP) continue;  // M31 has no four-step form
+        for (int split : {0, (int)SFNTT_PLAN_SPLIT12}) {
+          // the split changes nothing unless a layer range exceeds 12 layers
+          if (split && it.log_n + it.added_bits < 21) continue;
+          for (int one : {0, (int)SFNTT_PLAN_ONE_CTA}) plans.push_back(e | split | one);
+        }
+      }
+      plans.push_back(SFNTT_PLAN_TILE);
       for (int p : plans) {
-        if (it.field == SFNTT_M31 && p == SFNTT_PLAN_TMA_FOUR_STEP) continue;  // M31 has no four-step form
         it.plan = p;
         SFNTT_TRY(sfntt::run_item(ctx, it, s));  // warm
         SFNTT_CU(cudaEventRecord(ctx->ev_start, s));
@@ -339,7 +370,7 @@ int sfntt_tune_load(sfntt_ctx* ctx, const char* path) {
     std::istringstream is(line);
     std::string key;
     int plan = 0;
-    if (is >> key >> plan && plan >= SFNTT_PLAN_TMA && plan <= SFNTT_PLAN_TILE) ctx->tuned[key] = plan;
+    if (is >> key >> plan && plan != SFNTT_PLAN_AUTO && sfntt::valid_plan(plan)) ctx->tuned[key] = plan;
   }
   return done(ctx, {});
 }

@@ -105,11 +105,16 @@ struct ClusterNtt {
     const uint32_t base0 = rank * BASES + tid;  // group gi: base0 + gi NT
     uint32_t v[16];
     if constexpr (DESC) {
+      // Distributed shared memory may be written only once every block of the
+      // cluster is known to run: arrive here, wait just before the first
+      // remote store, so the barrier overlaps the loads and cross layers.
+      asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
 #pragma unroll
       for (int gi = 0; gi < GPT; ++gi)
 #pragma unroll
         for (int k = 0; k < G; ++k) v[gi * G + k] = col[base0 + (uint32_t)gi * NT + ((uint32_t)k << 12)];
       cross(v, base0, tw, 0u, 0u);
+      asm volatile("barrier.cluster.wait.aligned;" ::: "memory");
 #pragma unroll
       for (int gi = 0; gi < GPT; ++gi)
 #pragma unroll

@@ -121,6 +121,12 @@ struct sfntt_ctx {
   // for plain NTTs and the fused LDE.
   bool ntt_plain = SFNTT_NTT_PLAIN_DEFAULT;
   bool lde_plain = SFNTT_LDE_PLAIN_DEFAULT;
+  // Tuning knobs (autotuned plans): layer ranges above 12 layers split as a
+  // 12-layer contiguous pass plus the rest (instead of 8-layer strided passes
+  // plus the rest); persistent TMA passes launched with at most this many CTAs
+  // per SM (0: the kernel's own residency).
+  bool split_c12 = false;
+  int tma_ctas = 0;
   // autotuned plans: "field/log_n/columns/added_bits" -> sfntt_plan
   std::map<std::string, int> tuned;
 
@@ -177,6 +183,8 @@ Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d
 // inputs of a forward range or the outputs of an inverse range, indexed by
 // column position & edge_mask -- the boundary with an adjacent strided pass
 // run by another kernel.
+// Layer split of a TMA range [a, b) (ntt.cu): passes lo[i], cnt[i]; 0 = none.
+int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first);
 Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
                   uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
                   const uint2* tw, cudaStream_t stream, const uint2* edge_twist = nullptr,

@@ -196,7 +196,9 @@ Status launch_tma_expand(sfntt_ctx* ctx, const uint32_t* src, uint64_t src_strid
   auto kern = tma_expand_kernel<F, P, PLAIN, LSTAGE>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
-  const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)X::kCtasPerSm * (uint32_t)ctx->sm_count);
+  const uint32_t ctas =
+      ctx->tma_ctas > 0 ? std::min<uint32_t>((uint32_t)ctx->tma_ctas, (uint32_t)X::kCtasPerSm) : (uint32_t)X::kCtasPerSm;
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, ctas * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   SFNTT_CU(launch_pdl(kern, grid, X::NT, smem, s, pdl_fits(grid), min, mout, a));
   static const std::string name =

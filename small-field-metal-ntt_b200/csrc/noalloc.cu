@@ -17,8 +17,9 @@
 //   * the context's twiddle tables for (field, log_n) must already be resident
 //     (sfntt_prepare); the call never builds them (SFNTT_INVALID_ARGUMENT);
 //   * the first call on a device resolves the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it: make that
-//     first call before any stream capture;
+//     cudaGetSymbolAddress (with that device current) and caches it until the
+//     process exits: make that first call before any stream capture, and do
+//     not reset the device (cudaDeviceReset) while the library is loaded;
 //   * every call shares the one array and leaves its last contents there; each
 //     layer writes every word of its destination before any is read, so nothing
 //     needs clearing, but calls whose work overlaps on the GPU (different

@@ -12,11 +12,27 @@
 
 namespace sfntt {
 
-// TMA plan for layers [0, b): one contiguous pass of 5..12 layers, then
-// strided passes of 8 layers.
-static int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4]) {
+// TMA plan for layers [0, b): one contiguous pass, then strided passes of at
+// most 8 layers.  Default: the strided passes take 8 layers each and the
+// contiguous pass the rest (5..12 layers).  c12_first (a tuning knob, for
+// b > 12): the contiguous pass takes 12 layers and the strided passes share
+// the rest as evenly as possible (b = 14: 12 + 2 instead of 6 + 8).
+int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first) {
   if (a != 0) return 0;
   const uint32_t s = b > 12 ? (b - 12 + 7) / 8 : 0;
+  if (c12_first && s > 0) {
+    if (s > 3) return 0;
+    const uint32_t rest = b - 12;
+    lo[0] = 0;
+    cnt[0] = 12;
+    uint32_t at = 12;
+    for (uint32_t i = 1; i <= s; ++i) {
+      cnt[i] = rest / s + ((i - 1) < rest % s ? 1u : 0u);
+      lo[i] = at;
+      at += cnt[i];
+    }
+    return (int)(1 + s);
+  }
   const uint32_t c = b - 8 * s;
   if (c < 5 || c > 12 || s > 3) return 0;
   lo[0] = 0;
@@ -55,7 +71,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
                   const uint2* tw, cudaStream_t s, const uint2* edge_twist, uint32_t edge_mask) {
   uint32_t lo[4], cnt[4];
   if (!ctx->no_tma) {
-    const int kt = tma_split(a, b, lo, cnt);
+    const int kt = tma_split(a, b, lo, cnt, ctx->split_c12);
     TmaRequest req[4];
     bool ok = kt > 0;
     for (int i = 0; i < kt && ok; ++i) {
@@ -131,8 +147,11 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
 // One radix-2 layer over all columns: the per-layer dispatch of the
 // reference's V1 (src/ntt/*/metal_ct_dit_r2.rs) and, out of place, V3
 // (src/ntt/*/metal_stockham_r2.rs).  Same butterflies, same twiddles.
+// V1 and V2 run it in place (in == out), so in and out may alias: each thread
+// reads both points of its pair before it writes them, and no two threads
+// share a point.
 template <class F, bool DESC>
-__global__ void layer_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint2* __restrict__ tw,
+__global__ void layer_kernel(const uint32_t* in, uint32_t* out, const uint2* __restrict__ tw,
                              uint32_t log_n, uint32_t L, uint64_t pairs, uint32_t scale, uint32_t sw, uint32_t sws) {
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= pairs) return;

@@ -173,6 +173,22 @@ __device__ __forceinline__ void butterfly(uint32_t& a, uint32_t& b, uint2 w) {
   }
 }
 
+// The butterfly with twiddle 1 (same values and representation as
+// butterfly() with w = 1, whose Shoup product of x < 2p is x mod p).
+template <class F, bool DESC>
+__device__ __forceinline__ void butterfly_unit(uint32_t& a, uint32_t& b) {
+  if constexpr (Net<F, DESC>::kGS) {
+    const uint32_t s = add_mod<F>(a, b);
+    b = reduce2p<F>(a - b + F::P);
+    a = s;
+  } else {
+    const uint32_t ar = reduce2p<F>(a);
+    const uint32_t t = reduce2p<F>(b);
+    a = ar + t;
+    b = ar - t + F::P;
+  }
+}
+
 template <class F, bool DESC, Kind KD, int P, int LT, int R>
 struct Pass {
   static constexpr int CB = P + LT;

@@ -351,10 +351,34 @@ struct TPass {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
           if (m & (1 << j)) continue;
-          butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, tws, g, ct, m, b + j));
+          if (unit_twiddle<k>(m, b + j))  // a compile-time constant once the loops unroll
+            butterfly_unit<F, DESC>(v[m], v[m | (1 << j)]);
+          else
+            butterfly<F, DESC>(v[m], v[m | (1 << j)], twiddle<k>(a, tws, g, ct, m, b + j));
         }
       }
     }
+  }
+
+  // Staged passes index layer beta's twiddle by the group element's low beta
+  // bits (tw[beta][e mod 2^beta]).  Where none of round k's thread bits lies
+  // among those bits, the index is the slot's alone, and slots whose index is
+  // 0 multiply by tw[beta][0] = 1 (g^0 in the forward table and its inverse in
+  // the inverse one): their butterflies need no product.  In a 12-layer
+  // contiguous pass that is all of layer 0, half of layer 1, a quarter of
+  // layer 2 and an eighth of layer 3: 15 of each thread's 96 butterflies.
+  __host__ __device__ static constexpr uint32_t thread_tile_bits(int k) {
+    const RoundMap mp = make_map<KD, P, LT, R>(k);
+    uint32_t t = 0;
+    for (int g = 0; g < mp.ngrp; ++g) t |= mp.gmask[g] << mp.gshift[g];
+    return t;
+  }
+  template <int k>
+  __device__ static constexpr bool unit_twiddle(int m, int beta) {
+    if (!kStaged) return false;
+    constexpr int sh = (KD == Kind::C) ? 0 : 5;  // Kind::S: the group element sits above the 32 lanes
+    const uint32_t mask = (1u << beta) - 1u;
+    return ((thread_tile_bits(k) >> sh) & mask) == 0u && ((RM<KD, P, LT, R, k>::cm(m) >> sh) & mask) == 0u;
   }
 
   // ---- staging-buffer access in round k's layout ----

@@ -116,7 +116,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
-  const uint32_t grid = std::min<uint32_t>(a.ntiles, (uint32_t)T::kCtasPerSm * (uint32_t)ctx->sm_count);
+  const uint32_t ctas = ctx->tma_ctas > 0 ? std::min<uint32_t>((uint32_t)ctx->tma_ctas, T::kCtasPerSm) : T::kCtasPerSm;
+  const uint32_t grid = std::min<uint32_t>(a.ntiles, ctas * (uint32_t)ctx->sm_count);
   launch_begin(ctx, s);
   SFNTT_CU(launch_pdl(kern, grid, T::NT, smem, s, pdl_fits(grid), min, mout, a));
   return launch_check(ctx, tma_pass_name<F, DESC, KD, P, PLAIN, TW, LSTAGE>(), s,

@@ -556,6 +556,7 @@ def layout_dev(ctx: Context, in_ptr: int, out_ptr: int, log_n: int, batch: int, 
 
 # ------------------------------------------------------- uneven batches ---
 PLAN_AUTO, PLAN_TMA, PLAN_TMA_FOUR_STEP, PLAN_TILE = 0, 1, 2, 3
+PLAN_SPLIT12, PLAN_ONE_CTA = 4, 8  # flags on the TMA engines (layer split, one CTA per SM)
 
 
 class LdeBatch:
@@ -711,6 +712,14 @@ class Server:
     def pending(self) -> int:
         return int(_ffi.lib().sfntt_server_pending(self.handle))
 
+    def set_packing(self, max_requests: int) -> None:
+        """Up to max_requests queued requests of one shape share a launch as
+        columns of one batch (1: every request launches alone)."""
+        _check(self.ctx.handle, _ffi.lib().sfntt_server_set_packing(self.handle, max_requests))
+
+    def launches(self) -> int:
+        return int(_ffi.lib().sfntt_server_launches(self.handle))
+
     def close(self) -> None:
         if self.handle:
             _ffi.lib().sfntt_server_destroy(self.handle)
@@ -724,11 +733,14 @@ class Server:
 
 
 def serve_trace(ctx: Context, reqs: list[dict], arrivals, slots: int, budget_bytes: int,
-                host: list[tuple[np.ndarray, np.ndarray]] | None = None) -> tuple[np.ndarray, float]:
-    """Replays a trace (sfntt_serve_trace): request i submitted at arrivals[i]
-    seconds; returns (latency seconds per request, makespan seconds).  slots=1
-    is the plain sequential per-request loop.  `host`: per-request (input,
-    output) host arrays for host requests, else inputs at d_in on the device."""
+                host: list[tuple[np.ndarray, np.ndarray]] | None = None, max_pack: int = 1,
+                stats: dict | None = None) -> tuple[np.ndarray, float]:
+    """Replays a trace (sfntt_serve_trace_packed): request i submitted at
+    arrivals[i] seconds; returns (latency seconds per request, makespan
+    seconds).  slots=1 is the plain sequential per-request loop; max_pack > 1
+    lets up to that many same-shape requests share a launch.  `host`:
+    per-request (input, output) host arrays for host requests, else inputs at
+    d_in on the device.  `stats` (optional) receives the launch count."""
     n = len(reqs)
     arr = (_ffi.LdeItem * max(n, 1))()
     for i, it in enumerate(reqs):
@@ -741,8 +753,12 @@ def serve_trace(ctx: Context, reqs: list[dict], arrivals, slots: int, budget_byt
     if host is not None:
         h_in = (ctypes.c_void_p * max(n, 1))(*[h[0].ctypes.data for h in host])
         h_out = (ctypes.c_void_p * max(n, 1))(*[h[1].ctypes.data for h in host])
-    _check(ctx.handle, _ffi.lib().sfntt_serve_trace(ctx.handle, arr, h_in, h_out, t_arr.ctypes.data_as(dbl), n, slots,
-                                                    budget_bytes, lat.ctypes.data_as(dbl), ctypes.byref(mk)))
+    launches = ctypes.c_uint64()
+    _check(ctx.handle, _ffi.lib().sfntt_serve_trace_packed(ctx.handle, arr, h_in, h_out, t_arr.ctypes.data_as(dbl),
+                                                           n, slots, max_pack, budget_bytes, lat.ctypes.data_as(dbl),
+                                                           ctypes.byref(mk), ctypes.byref(launches)))
+    if stats is not None:
+        stats["launches"] = int(launches.value)
     return lat, mk.value
 
 

@@ -75,8 +75,12 @@ SIGNATURES = {
     "sfntt_server_result": (i32, [vp, u64, ctypes.POINTER(vp)]),
     "sfntt_server_release": (i32, [vp, u64]),
     "sfntt_server_pending": (sz, [vp]),
+    "sfntt_server_set_packing": (i32, [vp, i32]),
+    "sfntt_server_launches": (u64, [vp]),
     "sfntt_serve_trace": (i32, [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_double), sz, i32, sz,
                                 ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "sfntt_serve_trace_packed": (i32, [vp, vp, vp, vp, ctypes.POINTER(ctypes.c_double), sz, i32, i32, sz,
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), u64p]),
     "sfntt_host_alloc": (i32, [vp, sz, ctypes.POINTER(vp)]),
     "sfntt_host_free": (i32, [vp, vp]),
     "sfntt_launch_count": (u64, [vp]),

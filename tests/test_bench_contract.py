@@ -38,13 +38,14 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["e2e"]["value"] == d["value"]
-    assert "workload" in d["config"]
+    assert "workload" in d["config"] and d["config"]["parallelism"] == "single GPU"
+    assert d["step_stats"]["n"] == 1
 
 
 @pytest.mark.gpu
 def test_gpu_arm_prints_one_contract_line():
     r = _bench("--log-n", "14", "--batch", "16", "--steps", "3", "--warmup", "3", "--no-secondary", "--no-served",
-               "--cpu-seconds", "1", "--e2e-steps", "2", timeout=600)
+               "--no-uneven", "--cpu-seconds", "1", "--e2e-steps", "2", timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     lines = [l for l in r.stdout.splitlines() if l.strip()]
     assert len(lines) == 1, lines
@@ -59,3 +60,5 @@ def test_gpu_arm_prints_one_contract_line():
     assert {"value", "unit", "cores", "kind", "sample"} <= set(d["cpu_baseline"])
     assert d["e2e"]["h2d_bytes_per_step"] == 16 << 16 and d["e2e"]["d2h_bytes_per_step"] == 2 * (16 << 16)
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(d["clocks"])
+    st = d["step_stats"]
+    assert st["n"] == 3 and st["min_ms"] <= st["median_ms"] <= st["max_ms"] and st["cv_pct"] >= 0

@@ -40,11 +40,15 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
-    from sfntt import _ffi
-    out = subprocess.run(["cuobjdump", "--list-elf", str(_ffi.LIB_PATH)], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    """Every object of the library is compiled with the sm_100a target only
+    (no PTX to JIT elsewhere): the Makefile passes one -gencode, and every
+    compile and the link use it."""
+    mk = (ROOT / "small-field-metal-ntt_b200" / "Makefile").read_text()
+    arch = re.search(r"^ARCH\s*:=\s*(.+)$", mk, flags=re.M)
+    assert arch and arch.group(1).strip() == "-gencode arch=compute_100a,code=sm_100a"
+    assert re.search(r"^NVFLAGS\s*\?=.*\$\(ARCH\)", mk, flags=re.M)
+    assert "$(NVCC) $(NVFLAGS) -c" in mk and "$(NVCC) $(ARCH) -shared" in mk
+    assert "compute_" not in mk.replace("compute_100a", "")
 
 
 def test_status_strings_and_no_device_path():

@@ -62,7 +62,10 @@ def test_uneven_batch_plain_graph_tuned_match_oracle(ctx):
         assert np.array_equal(b[2].cpu().numpy().view(np.uint32), ref)
     batch.autotune(reps=1)
     plans = {batch.plan_of(i) for i in range(len(items))}
-    assert plans <= {sfntt.PLAN_TMA, sfntt.PLAN_TMA_FOUR_STEP, sfntt.PLAN_TILE} and plans
+    engines = {sfntt.PLAN_TMA, sfntt.PLAN_TMA_FOUR_STEP}
+    valid = {e | f for e in engines for f in (0, sfntt.PLAN_SPLIT12, sfntt.PLAN_ONE_CTA,
+                                              sfntt.PLAN_SPLIT12 | sfntt.PLAN_ONE_CTA)} | {sfntt.PLAN_TILE}
+    assert plans <= valid and plans
     for b in bufs:
         b[2].zero_()
     batch.run()
@@ -72,13 +75,23 @@ def test_uneven_batch_plain_graph_tuned_match_oracle(ctx):
     g.close()
 
 
-@pytest.mark.parametrize("plan", [sfntt.PLAN_TMA, sfntt.PLAN_TMA_FOUR_STEP, sfntt.PLAN_TILE])
+@pytest.mark.parametrize("plan", [sfntt.PLAN_TMA, sfntt.PLAN_TMA_FOUR_STEP, sfntt.PLAN_TILE,
+                                  sfntt.PLAN_TMA | sfntt.PLAN_SPLIT12, sfntt.PLAN_TMA_FOUR_STEP | sfntt.PLAN_SPLIT12,
+                                  sfntt.PLAN_TMA | sfntt.PLAN_ONE_CTA,
+                                  sfntt.PLAN_TMA_FOUR_STEP | sfntt.PLAN_SPLIT12 | sfntt.PLAN_ONE_CTA])
 def test_every_plan_is_exact(ctx, plan):
+    """Every engine and knob, on shapes where the layer split differs (a
+    layer range of 13..14 layers: 12 + 1..2 against 5..6 + 8)."""
     import torch
     items = [{"field": sfntt.FIELD_BABYBEAR, "log_n": 14, "batch": 3, "added_bits": 2, "plan": plan},
              {"field": sfntt.FIELD_BABYBEAR, "log_n": 16, "batch": 2, "added_bits": 0, "plan": plan},
-             {"field": sfntt.FIELD_M31, "log_n": 15, "batch": 2, "added_bits": 1, "plan": plan}]
+             {"field": sfntt.FIELD_M31, "log_n": 15, "batch": 2, "added_bits": 1, "plan": plan},
+             {"field": sfntt.FIELD_BABYBEAR, "log_n": 21, "batch": 1, "added_bits": 1, "plan": plan},
+             {"field": sfntt.FIELD_BABYBEAR, "log_n": 22, "batch": 1, "added_bits": 0, "plan": plan},
+             {"field": sfntt.FIELD_M31, "log_n": 22, "batch": 1, "added_bits": 1, "plan": plan}]
     bufs = _alloc(items, 900 + plan)
+    with pytest.raises(sfntt.InvalidArgument):
+        sfntt.LdeBatch(ctx, [dict(items[0], plan=16)]).run()
     batch = sfntt.LdeBatch(ctx, items)
     batch.prepare()
     batch.run()

@@ -148,3 +148,75 @@ def test_trace_replay_device_inputs(ctx):
     for lat in (lat_plain, lat_srv):
         assert np.all(lat > 0) and np.all(np.isfinite(lat))
     assert mk_plain >= arrivals[-1] and mk_srv >= arrivals[-1]
+
+
+def _small_same_shape_mix(seed):
+    """Requests of three shapes (both fields), interleaved, small enough that
+    several share the GPU: packing candidates."""
+    rng = np.random.default_rng(seed)
+    shapes = [(sfntt.FIELD_BABYBEAR, 13, 1), (sfntt.FIELD_M31, 14, 2), (sfntt.FIELD_BABYBEAR, 12, 2)]
+    reqs = []
+    for i in range(24):
+        f, ln, ab = shapes[i % 3]
+        reqs.append({"field": f, "log_n": ln, "batch": int(rng.integers(1, 6)), "added_bits": ab})
+    return reqs
+
+
+def test_packed_requests_same_alone_and_in_one_launch(ctx):
+    """With packing, queued requests of one shape run as the columns of one
+    batch: every request's output equals its plain drop-in call and the
+    oracle, device and host requests mixed, and the launches are fewer than
+    the requests."""
+    import torch
+    reqs = _small_same_shape_mix(3)
+    xs = [_input(it, 2100 + i) for i, it in enumerate(reqs)]
+    d_ins = [torch.from_numpy(x.view(np.int32).copy()).cuda() for x in xs]
+    srv = sfntt.Server(ctx, budget_bytes=512 << 20, slots=2)
+    srv.set_packing(16)
+    tickets, host_out = {}, {}
+    for i, (it, d) in enumerate(zip(reqs, d_ins)):
+        if i % 4 == 3:  # every fourth request comes from the host
+            t, out = srv.submit_host(it, xs[i])
+            host_out[i] = out
+        else:
+            it["d_in"] = d.data_ptr()
+            t = srv.submit(it)
+        tickets[t] = i
+    got = {}
+    while len(got) < len(reqs):
+        for t in srv.poll():
+            i = tickets[t]
+            it = reqs[i]
+            if i in host_out:
+                got[i] = host_out[i]
+            else:
+                got[i] = srv.result(t, it["batch"] << (it["log_n"] + it["added_bits"])).cpu().numpy() \
+                    .view(np.uint32).copy()
+            srv.release(t)
+    launches = srv.launches()
+    assert srv.pending() == 0
+    srv.close()
+    assert launches < len(reqs), launches
+    for i, (it, x, d) in enumerate(zip(reqs, xs, d_ins)):
+        alone = _alone(ctx, it, d)
+        assert np.array_equal(got[i], alone), (i, it)
+        assert np.array_equal(alone, _oracle(it, x)), (i, it)
+
+
+@pytest.mark.parametrize("max_pack", [1, 8])
+def test_trace_replay_packed_host_outputs_exact(ctx, max_pack):
+    reqs, arrivals = sfntt.served_workload(32, rate=20000.0, seed=8, cols_range=(1, 4),
+                                           log_n_weights={13: 1, 14: 1})
+    host = []
+    for i, it in enumerate(reqs):
+        x = _input(it, 1700 + i)
+        host.append((x, np.zeros(it["batch"] << (it["log_n"] + it["added_bits"]), dtype=np.uint32)))
+    stats = {}
+    lat, makespan = sfntt.serve_trace(ctx, reqs, arrivals, slots=4, budget_bytes=256 << 20, host=host,
+                                      max_pack=max_pack, stats=stats)
+    assert np.all(lat > 0) and np.all(np.isfinite(lat))
+    assert stats["launches"] <= len(reqs)
+    if max_pack == 1:
+        assert stats["launches"] == len(reqs)
+    for it, (x, out) in zip(reqs, host):
+        assert np.array_equal(out, _oracle(it, x)), it
