@@ -127,6 +127,9 @@ struct sfntt_ctx {
   // per SM (0: the kernel's own residency).
   bool split_c12 = false;
   int tma_ctas = 0;
+  // contiguous 8- and 12-layer TMA passes run their two CTA halves as
+  // independent pipelines (half tiles, own barriers); off: whole tiles
+  bool c_halves = false;
   // autotuned plans: "field/log_n/columns/added_bits" -> sfntt_plan
   std::map<std::string, int> tuned;
 

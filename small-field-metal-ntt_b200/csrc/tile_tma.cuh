@@ -86,7 +86,8 @@ struct TileCoord {
 // per-position twiddles): the caller has staged the twiddles of the tile's
 // 32-position chunk in shared memory (see lchunk_entry), so every twiddle is a
 // shared-memory load instead of an L2 one.
-template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false, bool LSTAGE = false>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN = false, bool TW = false, bool LSTAGE = false,
+          bool HALVES = false>
 struct TPass {
   // LSTAGE: each CTA takes a contiguous range of tiles ordered so that it
   // stays on one set of positions across the columns, and stages that set's
@@ -590,7 +591,102 @@ struct TPass {
     }
   }
 
+  // ---- independent halves (contiguous passes whose rounds all have R layers) ----
+  // Tile bit CB-1 is then thread bit log2(NT)-1 in every round, so the two
+  // halves of the CTA (256 threads each) work on the two 2^(CB-1)-word halves
+  // of a tile without ever exchanging data.  run_halves gives each half its
+  // own TMA pipeline (half tiles of 16 KiB, double-buffered, its own
+  // mbarriers, its own store) and its own pre-store barrier, so a half never
+  // waits for the other: the CTA-wide barriers, and the phase lock-step they
+  // impose on all 16 warps, are gone.
+  __host__ __device__ static constexpr bool halves_ok() {
+    if (KD != Kind::C || LSTAGE || NT != 512) return false;
+    for (int k = 0; k < K; ++k)
+      if (tid_bit(k, CB - 1) != 8) return false;
+    return true;
+  }
+  static_assert(!HALVES || halves_ok(), "independent halves: contiguous tiles whose top bit is thread bit 8");
+  static constexpr uint32_t HWORDS = TWORDS / 2, HBYTES = TBYTES / 2, HROWS = HWORDS / 32;
+
+  __device__ static void run_halves(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
+    extern __shared__ __align__(1024) uint32_t smem_words[];
+    const uint32_t tid = threadIdx.x;
+    const uint32_t half = tid >> 8;
+    const bool leader = (tid & 255u) == 0u;
+    uint32_t* stage = smem_words + half * 2u * HWORDS;  // this half's two half-tile buffers
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem_words + 2 * TWORDS) + 2u * half;
+    uint2* tws = reinterpret_cast<uint2*>(reinterpret_cast<uint64_t*>(smem_words + 2 * TWORDS) + 4);
+    const TmaArgs& a = args;
+    uint32_t t = blockIdx.x;
+    const uint32_t t_end = a.ntiles, t_step = gridDim.x;
+    if (t >= t_end) return;
+    if constexpr (kStaged) stage_twiddles(tws, a.tw, tid);
+    if (leader) {
+      tma::prefetch_map(min);
+      tma::prefetch_map(mout);
+      tma::mbar_init(&bar[0], 1);
+      tma::mbar_init(&bar[1], 1);
+      tma::fence_mbar_init();
+    }
+    __syncthreads();  // staged twiddles and barriers: the halves' last shared step
+    const int32_t hrow = (int32_t)(half * HROWS);
+    if (leader) {
+      const Geo g0 = geo(a, t);
+      tma::mbar_expect_tx(&bar[0], HBYTES);
+      tma::load_3d(stage, min, 0, g0.c1 + hrow, g0.c2, &bar[0]);
+    }
+    const uint32_t bar_id = 3u + half;  // named barriers 1, 2 are the rounds' exchanges
+    uint32_t v[E];
+    for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
+      const uint32_t buf = it & 1u;
+      uint32_t* cur = stage + buf * HWORDS;
+      // tile word c of this half (bit CB-1 = half) sits at view + sw(c) = cur + sw(c mod 2^(CB-1))
+      uint32_t* view = cur - half * HWORDS;
+      const uint32_t tn = t + t_step;
+      if (leader && tn < t_end) {
+        tma::wait_reads();  // the store that last used the other buffer has read it
+        const Geo gn = geo(a, tn);
+        tma::mbar_expect_tx(&bar[buf ^ 1u], HBYTES);
+        tma::load_3d(stage + (buf ^ 1u) * HWORDS, min, 0, gn.c1 + hrow, gn.c2, &bar[buf ^ 1u]);
+      }
+      const Geo g = geo(a, t);
+      const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      ld<kFirst>(view, v, tid);
+      if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
+      rounds<0>(view, v, a, tws, g, tid);
+      finish(v, a, g, tid);
+      st<kLast>(view, v, tid);
+      tma::fence_proxy_async();
+      uint32_t any_bad;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\t"
+          "setp.ne.u32 p, %1, 0;\n\t"
+          "bar.red.or.pred q, %2, 256, p;\n\t"
+          "selp.u32 %0, 1, 0, q;\n\t}"
+          : "=r"(any_bad)
+          : "r"(ok ? 0u : 1u), "r"(bar_id)
+          : "memory");
+      if (any_bad) {
+        if (leader) {
+          atomicExch(a.err, 1);
+          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          tma::wait_all();
+        }
+        return;
+      }
+      if (leader) {
+        tma::store_3d(mout, 0, g.c1 + hrow, g.c2, cur);
+        tma::commit();
+      }
+    }
+    if (leader) tma::wait_all();
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
+    if constexpr (HALVES) {
+      run_halves(min, mout, args);
+      return;
+    }
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
     extern __shared__ __align__(1024) uint32_t smem_words[];
@@ -692,12 +788,12 @@ static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: l
 
 // BabyBear LSTAGE passes stage 64 KiB of twiddles besides the two tiles (one
 // CTA per SM); M31 contiguous ones 32 KiB (two).
-template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false>
-__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::NT,
-                                  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::kCtasPerSm)
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false, bool HALVES = false>
+__global__ void __launch_bounds__(TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>::NT,
+                                  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>::kCtasPerSm)
 tma_pass_kernel(const __grid_constant__ CUtensorMap min, const __grid_constant__ CUtensorMap mout, TmaArgs a) {
   pdl_enter();
-  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>::run(&min, &mout, a);
+  TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>::run(&min, &mout, a);
 }
 
 // ---------------------------------------------------------------------------

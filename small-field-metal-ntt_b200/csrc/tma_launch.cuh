@@ -51,10 +51,13 @@ inline bool tma_pass_ok(const TmaRequest& r) {
   return r.P >= 1 && r.P <= 8 && r.lo >= 5 && r.lo + r.P <= r.log_n;
 }
 
-inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n, uint64_t stride, uint32_t batch) {
+// box_rows: 128-byte rows per copy (a whole 2^13-word tile, or half of one
+// for passes that run independent halves).
+inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n, uint64_t stride, uint32_t batch,
+                           uint32_t box_rows = kTileWords / 32) {
   const uint64_t n = 1ull << log_n;
   cuuint64_t dims[3], strides[2];
-  const cuuint32_t box[3] = {32, kTileWords / 32, 1};
+  const cuuint32_t box[3] = {32, box_rows, 1};
   if (n >= kTileWords) {
     dims[0] = 32; dims[1] = n / 32; dims[2] = batch;
     strides[0] = 128; strides[1] = stride * 4;
@@ -82,9 +85,9 @@ const char* tma_pass_name() {
   return nm.c_str();
 }
 
-template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false>
+template <class F, bool DESC, Kind KD, int P, bool PLAIN, bool TW, bool LSTAGE = false, bool HALVES = false>
 Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
-  using T = TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
+  using T = TPass<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>;
   const uint64_t n = 1ull << r.log_n;
   CUtensorMap min, mout;
   TmaArgs a{};
@@ -99,8 +102,9 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   a.twist = r.twist;
   a.twist_mask = r.twist_mask;
   if constexpr (KD == Kind::C) {
-    SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch));
-    SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch));
+    const uint32_t rows = HALVES ? T::HROWS : kTileWords / 32;
+    SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch, rows));
+    SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch, rows));
     a.spans = n < kTileWords;
     a.log_tpc = a.spans ? 0u : r.log_n - kTileBits;
     // every M31 table with n >= 2^13 carries its first-round copy from entry n on
@@ -112,8 +116,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
   }
-  constexpr int smem = 2 * (int)T::TBYTES + 16 + (int)T::SMEM_TW_BYTES + 1024;
-  auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE>;
+  constexpr int smem = 2 * (int)T::TBYTES + 32 + (int)T::SMEM_TW_BYTES + 1024;
+  auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
   const uint32_t ctas = ctx->tma_ctas > 0 ? std::min<uint32_t>((uint32_t)ctx->tma_ctas, T::kCtasPerSm) : T::kCtasPerSm;
@@ -128,11 +132,17 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
 #define SFNTT_TMA_C(PP)                                                                          \
   case PP:                                                                                       \
     if constexpr (F::kMontgomery) {                                                              \
-      if (r.twist) return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);         \
+      if (r.twist) {                                                                             \
+        if constexpr (TPass<F, DESC, Kind::C, PP, false, true>::halves_ok())                     \
+          if (ctx->c_halves) return launch_tma_pass<F, DESC, Kind::C, PP, false, true, false, true>(ctx, r, s); \
+        return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);                    \
+      }                                                                                          \
     } else if constexpr (PP == 12) {                                                             \
       if (r.lstage && r.log_n >= kTileBits)                                                      \
         return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);             \
     }                                                                                            \
+    if constexpr (TPass<F, DESC, Kind::C, PP, false, false>::halves_ok())                        \
+      if (ctx->c_halves) return launch_tma_pass<F, DESC, Kind::C, PP, false, false, false, true>(ctx, r, s); \
     return launch_tma_pass<F, DESC, Kind::C, PP, false, false>(ctx, r, s);
 #define SFNTT_TMA_S(PP)                                                                          \
   case PP:                                                                                       \
