@@ -469,7 +469,7 @@ def headline_keys(secondary, uneven, served) -> dict:
             out[f"bb_2^{k}_fwd_inv_us"] = secondary["bb"][k]["fwd_inv_us"]
         out["bb_2^24_gelem_s"] = secondary["bb"]["24"]["gelem_s"]
     if uneven:
-        for k in ("plain_loop_ms", "graph_ms", "persistent_ms", "speedup", "persistent_speedup"):
+        for k in ("plain_loop_ms", "graph_ms", "persistent_ms", "speedup", "persistent_speedup", "persistent_vs_graph"):
             if k in uneven:
                 out[f"uneven_{k}"] = uneven[k]
     if served:
@@ -797,7 +797,9 @@ def uneven_metrics(a, ctx, sfntt, torch) -> dict:
     """The uneven-batch configuration: 64 polynomials, field 50/50 M31 /
     BabyBear, log n uniform in 12..22, 1..128 columns, blow-up 1/2/4 with
     probability 1/3 each, seeded; one plain launch sequence per polynomial vs
-    one autotuned CUDA-graph launch for the whole batch, outputs compared."""
+    one autotuned CUDA-graph launch for the whole batch (per-item kernels on 8
+    lanes) vs the persistent form (one work-list launch per LDE phase for every
+    2^13..2^20-point item, the rest per item beside it), outputs compared."""
     items = sfntt.uneven_workload(64, seed=2024)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(99)
@@ -842,11 +844,22 @@ def uneven_metrics(a, ctx, sfntt, torch) -> dict:
     g = batch.graph(lanes=a.lanes)
     graph_ms = timed(lambda: g.launch(stream), steps)
     d_graph = digest()
+    # persistent form: the eligible items' three phases as one work-list launch each
+    for _, y in keep:
+        y.zero_()
+    pg = batch.persistent_graph(lanes=a.lanes)
+    persistent_ms = timed(lambda: pg.launch(stream), steps)
+    d_persistent = digest()
+    persistent_kernels = pg.kernel_count()
+    pg.close()
     elems_out = sum(it["batch"] << (it["log_n"] + it["added_bits"]) for it in items)
     bytes_alg = sum(4 * (it["batch"] << it["log_n"]) * (1 + (1 << it["added_bits"])) for it in items)
     peak, peak_kind = peaks()
     line = {"metric": "uneven batch: 64 mixed M31/BabyBear LDEs", "unit": "ms", "value": graph_ms,
             "plain_loop_ms": plain_ms, "graph_ms": graph_ms, "speedup": plain_ms / graph_ms,
+            "persistent_ms": persistent_ms, "persistent_speedup": plain_ms / persistent_ms,
+            "persistent_vs_graph": graph_ms / persistent_ms, "kernels_in_persistent_graph": persistent_kernels,
+            "persistent_outputs_identical": d_plain == d_persistent,
             "higher_is_better": False, "steps": steps, "warmup": a.warmup, "lanes": a.lanes,
             "kernels_in_graph": g.kernel_count(), "outputs_identical": d_plain == d_graph,
             "melem_per_s_out": elems_out / (graph_ms * 1e-3) / 1e6,

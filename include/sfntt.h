@@ -262,6 +262,17 @@ int sfntt_batch_run(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, v
  * overlap.  Replay with sfntt_graph_launch: one launch for the batch. */
 int sfntt_batch_graph_create(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int lanes,
                              sfntt_graph **out);
+/* The same batch in persistent form: every BabyBear / M31 item with
+ * 2^13..2^20 points, blow-up <= 16 and the default plan runs its LDE in three
+ * phases -- inverse low layers, expansion, forward low layers -- and each
+ * phase is ONE persistent launch over all those items: its CTAs pop (item,
+ * tile range) units from a work list in device memory (owned by the graph)
+ * and keep the next tile's TMA load in flight across item boundaries.  The
+ * other items run their own launches on `lanes` forked streams beside the
+ * phases.  Outputs are identical to the per-item launches.  (The reference
+ * dispatches one grid per layer group per batch, src/ntt/babybear/batch.rs:76-180.) */
+int sfntt_batch_persistent_create(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int lanes,
+                                  sfntt_graph **out);
 int sfntt_graph_launch(sfntt_graph *graph, void *stream);
 uint64_t sfntt_graph_kernel_count(const sfntt_graph *graph);
 void sfntt_graph_destroy(sfntt_graph *graph);

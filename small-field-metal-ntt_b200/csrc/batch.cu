@@ -27,12 +27,14 @@
 
 #include "context.hpp"
 #include "host_field.hpp"
+#include "worklist.cuh"
 
 struct sfntt_graph {
   int device = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t kernels = 0;
+  void* work = nullptr;  // persistent form: the device work lists and their counters
 };
 
 namespace sfntt {
@@ -281,6 +283,116 @@ int sfntt_batch_graph_create(sfntt_ctx* ctx, const sfntt_lde_item* items, size_t
   return done(ctx, {});
 }
 
+int sfntt_batch_persistent_create(sfntt_ctx* ctx, const sfntt_lde_item* items, size_t count, int lanes,
+                                  sfntt_graph** out) {
+  if (!ctx || !out || (count && !items)) return SFNTT_INVALID_ARGUMENT;
+  Guard g(ctx);
+  *out = nullptr;
+  if (lanes < 1) lanes = 1;
+  if (lanes > 32) lanes = 32;
+  std::vector<cudaStream_t> lane(lanes + 1, nullptr);  // lane[0]: the persistent phases
+  std::vector<cudaEvent_t> join(lanes + 1, nullptr);
+  cudaEvent_t fork = nullptr;
+  cudaStream_t origin = nullptr;
+  auto* gr = new sfntt_graph();
+  gr->device = ctx->device;
+  auto build = [&]() -> Status {
+    for (size_t i = 0; i < count; ++i) SFNTT_TRY(sfntt::prepare_item(ctx, items[i], ctx->stream));
+    SFNTT_CU(cudaStreamSynchronize(ctx->stream));
+    // the work lists of the three phases (tables are final: every item is prepared)
+    sfntt::WorkPhase ph[sfntt::kWorkPhases];
+    std::vector<size_t> rest;
+    for (size_t i = 0; i < count; ++i) {
+      if (!sfntt::worklist_eligible(ctx, items[i])) {
+        rest.push_back(i);
+        continue;
+      }
+      for (int p = 0; p < sfntt::kWorkPhases; ++p) SFNTT_TRY(sfntt::worklist_add(ctx, ph[p], p, items[i], ctx->stream));
+    }
+    // one device block: counters, then per phase its items (128-byte aligned) and units
+    size_t off = 256, item_off[sfntt::kWorkPhases], unit_off[sfntt::kWorkPhases];
+    for (int p = 0; p < sfntt::kWorkPhases; ++p) {
+      item_off[p] = off;
+      off += (ph[p].items.size() * sizeof(sfntt::WorkItem) + 255) & ~size_t(255);
+      unit_off[p] = off;
+      off += (ph[p].units.size() * sizeof(sfntt::WorkUnit) + 255) & ~size_t(255);
+    }
+    SFNTT_CU(cudaMalloc(&gr->work, off));
+    uint8_t* base = static_cast<uint8_t*>(gr->work);
+    SFNTT_CU(cudaMemset(base, 0, 256));
+    for (int p = 0; p < sfntt::kWorkPhases; ++p) {
+      if (!ph[p].items.empty())
+        SFNTT_CU(cudaMemcpy(base + item_off[p], ph[p].items.data(), ph[p].items.size() * sizeof(sfntt::WorkItem),
+                            cudaMemcpyHostToDevice));
+      if (!ph[p].units.empty())
+        SFNTT_CU(cudaMemcpy(base + unit_off[p], ph[p].units.data(), ph[p].units.size() * sizeof(sfntt::WorkUnit),
+                            cudaMemcpyHostToDevice));
+    }
+    uint32_t* counters = reinterpret_cast<uint32_t*>(base);
+    SFNTT_CU(cudaStreamCreateWithFlags(&origin, cudaStreamNonBlocking));
+    SFNTT_CU(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int l = 0; l <= lanes; ++l) {
+      SFNTT_CU(cudaStreamCreateWithFlags(&lane[l], cudaStreamNonBlocking));
+      SFNTT_CU(cudaEventCreateWithFlags(&join[l], cudaEventDisableTiming));
+    }
+    const uint64_t k0 = ctx->launches.load();
+    SFNTT_CU(cudaStreamBeginCapture(origin, cudaStreamCaptureModeThreadLocal));
+    Status st = [&]() -> Status {
+      SFNTT_CU(cudaEventRecord(fork, origin));
+      for (int l = 0; l <= lanes; ++l) SFNTT_CU(cudaStreamWaitEvent(lane[l], fork, 0));
+      // lane 0: the three persistent phases, each one launch over every eligible item
+      SFNTT_CU(cudaMemsetAsync(counters, 0, sfntt::kWorkPhases * sizeof(uint32_t), lane[0]));
+      for (int p = 0; p < sfntt::kWorkPhases; ++p)
+        SFNTT_TRY(sfntt::worklist_launch(ctx, p, ph[p], reinterpret_cast<const sfntt::WorkItem*>(base + item_off[p]),
+                                         reinterpret_cast<const sfntt::WorkUnit*>(base + unit_off[p]), counters + p,
+                                         lane[0]));
+      // the other items: per-item launches, largest first to the least-loaded lane
+      auto work = [&](size_t i) {
+        return (double)items[i].batch * (double)(1ull << items[i].log_n) * (1.0 + (double)(1u << items[i].added_bits));
+      };
+      std::stable_sort(rest.begin(), rest.end(), [&](size_t a, size_t b) { return work(a) > work(b); });
+      std::vector<double> load(lanes, 0.0);
+      for (size_t i : rest) {
+        int best = 0;
+        for (int l = 1; l < lanes; ++l)
+          if (load[l] < load[best]) best = l;
+        load[best] += work(i);
+        SFNTT_TRY(sfntt::run_item(ctx, items[i], lane[1 + best]));
+      }
+      for (int l = 0; l <= lanes; ++l) {
+        SFNTT_CU(cudaEventRecord(join[l], lane[l]));
+        SFNTT_CU(cudaStreamWaitEvent(origin, join[l], 0));
+      }
+      return {};
+    }();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(origin, &graph);
+    if (!st.ok()) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    SFNTT_CU(e);
+    gr->graph = graph;
+    gr->kernels = ctx->launches.load() - k0;
+    SFNTT_CU(cudaGraphInstantiate(&gr->exec, graph, 0));
+    return {};
+  };
+  Status s = build();
+  for (int l = 0; l <= lanes; ++l) {
+    if (lane[l]) cudaStreamDestroy(lane[l]);
+    if (join[l]) cudaEventDestroy(join[l]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (origin) cudaStreamDestroy(origin);
+  if (!s.ok()) {
+    sfntt_graph_destroy(gr);
+    cudaGetLastError();
+    return done(ctx, s);
+  }
+  *out = gr;
+  return done(ctx, {});
+}
+
 int sfntt_graph_launch(sfntt_graph* g, void* stream) {
   if (!g || !g->exec) return SFNTT_INVALID_ARGUMENT;
   int prev = -1;
@@ -300,6 +412,7 @@ void sfntt_graph_destroy(sfntt_graph* g) {
   if (prev != g->device) cudaSetDevice(g->device);
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->work) cudaFree(g->work);
   if (prev >= 0 && prev != g->device) cudaSetDevice(prev);
   delete g;
 }

@@ -591,6 +591,18 @@ struct TPass {
     }
   }
 
+  // One tile in shared memory, in place: the first round's load, every round,
+  // the finish and the last round's store (the work-list kernels' tile step).
+  __device__ static __forceinline__ void tile_body(uint32_t* cur, const TmaArgs& a, const uint2* tws, const Geo& g,
+                                                   uint32_t tid) {
+    uint32_t v[E];
+    ld<kFirst>(cur, v, tid);
+    if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
+    rounds<0>(cur, v, a, tws, g, tid);
+    finish(v, a, g, tid);
+    st<kLast>(cur, v, tid);
+  }
+
   // ---- independent halves (contiguous passes whose rounds all have R layers) ----
   // Tile bit CB-1 is then thread bit log2(NT)-1 in every round, so the two
   // halves of the CTA (256 threads each) work on the two 2^(CB-1)-word halves
@@ -600,10 +612,9 @@ struct TPass {
   // waits for the other: the CTA-wide barriers, and the phase lock-step they
   // impose on all 16 warps, are gone.
   __host__ __device__ static constexpr bool halves_ok() {
-    if (KD != Kind::C || LSTAGE || NT != 512) return false;
-    for (int k = 0; k < K; ++k)
-      if (tid_bit(k, CB - 1) != 8) return false;
-    return true;
+    bool ok = KD == Kind::C && !LSTAGE && NT == 512;
+    for (int k = 0; k < K && ok; ++k) ok = tid_bit(k, CB - 1) == 8;
+    return ok;
   }
   static_assert(!HALVES || halves_ok(), "independent halves: contiguous tiles whose top bit is thread bit 8");
   static constexpr uint32_t HWORDS = TWORDS / 2, HBYTES = TBYTES / 2, HROWS = HWORDS / 32;
@@ -831,6 +842,80 @@ struct TExpand {
     for (int m = 0; m < E; ++m) w[m] = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
   }
 
+  // LSTAGE: the 32-position chunk of tile t, whose per-position twiddles the
+  // tile reads from shared memory (tiles are numbered column-fastest).
+  __device__ static __forceinline__ uint32_t chunk_of(const TmaArgs& ai, uint32_t t) {
+    return (t / ai.batch) & ((1u << (ai.lo - 5)) - 1u);
+  }
+
+  // One input tile (in `cur`; ok: it arrived) through the inverse layers, then
+  // for every output block q the multipliers and forward layers, each block
+  // leaving with its own TMA store (block 0 from cur, block 1 from ostage,
+  // alternating).  A wait that ran out is agreed on at the barrier before the
+  // first store (the inverse and the first block touch only in-bounds shared
+  // memory, twiddles and multipliers whatever the tile holds): then nothing is
+  // stored and the result is false.
+  __device__ static __forceinline__ bool tile_body(uint32_t* cur, uint32_t* ostage, const TmaArgs& ai,
+                                                   const uint2* tws_inv, const uint2* tws_fwd, uint32_t t, bool ok,
+                                                   const CUtensorMap* mout, uint32_t tid) {
+    using M = RM<Kind::S, P, LT, R, K - 1>;
+    const uint32_t ct = M::ctid(tid);
+    const uint32_t lo = ai.lo;
+    const uint32_t n = 1u << ai.log_n;
+    const uint32_t nq = 1u << ai.log_q;
+    uint32_t x[E], v[E];
+    const typename Inv::Geo g = Inv::geo(ai, t);
+    // position of slot m: pos_base + u + (e << lo)
+    const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
+    // BabyBear multipliers are software-pipelined: block q+1's are loaded
+    // while block q's forward layers run (block 0's during the inverse).
+    uint2 w[F::kMontgomery ? E : 1];
+    if constexpr (F::kMontgomery) load_mul(w, ai.mul + pos_t, lo);
+    Inv::template ld<0>(cur, x, tid);
+    Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
+    if constexpr (!F::kMontgomery) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) x[m] = mul_shoup<F>(x[m], ai.scale_w, ai.scale_ws);  // n^-1
+    }
+    for (uint32_t q = 0; q < nq; ++q) {
+      uint32_t* ob = (q & 1u) ? ostage : cur;
+      // The TMA store that last read ob is the one before the newest pending
+      // store (for q = 1: the previous tile's last ostage store, which no
+      // prefetch wait covers on a CTA's last tile).
+      if (q >= 1) {
+        if (tid == 0) tma::wait_reads_1();
+        __syncthreads();
+      }
+      if constexpr (F::kMontgomery) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
+        if (q + 1 < nq) load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);
+      } else {
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = x[m];
+      }
+      typename Inv::Geo gq = g;
+      gq.hb = q;  // high block of the extended network (M31 per-block twiddles)
+      Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, gq, tid);  // forward starts in round K-1's layout
+      if constexpr (!Net<F, true>::kGS) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = reduce2p<F>(v[m]);  // lazy CT values to [0, p)
+      }
+      Fwd::template st<0>(ob, v, tid);
+      tma::fence_proxy_async();
+      if (q == 0) {
+        if (__syncthreads_or(!ok)) return false;
+      } else {
+        __syncthreads();
+      }
+      if (tid == 0) {
+        tma::store_5d(mout, 0, g.s1, 0, (int32_t)q, g.s4, ob);
+        tma::commit();
+      }
+    }
+    return true;
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
@@ -870,12 +955,6 @@ struct TExpand {
       tma::mbar_expect_tx(&bar[0], TBYTES);
       Inv::tma_load(min, Inv::geo(ai, t), stage, &bar[0]);
     }
-    using M = RM<Kind::S, P, LT, R, K - 1>;
-    const uint32_t ct = M::ctid(tid);
-    const uint32_t lo = ai.lo;
-    const uint32_t n = 1u << ai.log_n;
-    const uint32_t nq = 1u << ai.log_q;
-    uint32_t x[E], v[E];
     uint32_t staged = ~0u;  // chunk whose twiddles are in shared memory (LSTAGE)
     for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
       const uint32_t buf = it & 1u;
@@ -890,7 +969,7 @@ struct TExpand {
         // Every thread passed the previous tile's last barrier after its last
         // twiddle read; the barrier here publishes the new copy (the chunk,
         // a function of t, is the same for the whole CTA).
-        const uint32_t chunk = (t / ai.batch) & ((1u << (ai.lo - 5)) - 1u);
+        const uint32_t chunk = chunk_of(ai, t);
         if (chunk != staged) {
           Inv::stage_lchunk(tws_inv, ai.tw, ai.lo, chunk, tid);
           Fwd::stage_lchunk(tws_fwd, ai.tw_fwd, ai.lo, chunk, tid);
@@ -898,65 +977,14 @@ struct TExpand {
           __syncthreads();
         }
       }
-      // A wait that ran out is agreed on at the barrier before the first
-      // store (the inverse and the first block touch only in-bounds shared
-      // memory, twiddles and multipliers whatever the tile holds).
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
-      const typename Inv::Geo g = Inv::geo(ai, t);
-      // position of slot m: pos_base + u + (e << lo)
-      const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
-      // BabyBear multipliers are software-pipelined: block q+1's are loaded
-      // while block q's forward layers run (block 0's during the inverse).
-      uint2 w[F::kMontgomery ? E : 1];
-      if constexpr (F::kMontgomery) load_mul(w, ai.mul + pos_t, lo);
-      Inv::template ld<0>(cur, x, tid);
-      Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
-      if constexpr (!F::kMontgomery) {
-#pragma unroll
-        for (int m = 0; m < E; ++m) x[m] = mul_shoup<F>(x[m], ai.scale_w, ai.scale_ws);  // n^-1
-      }
-      for (uint32_t q = 0; q < nq; ++q) {
-        uint32_t* ob = (q & 1u) ? ostage : cur;
-        // The TMA store that last read ob is the one before the newest pending
-        // store (for q = 1: the previous tile's last ostage store, which no
-        // prefetch wait covers on a CTA's last tile).
-        if (q >= 1) {
-          if (tid == 0) tma::wait_reads_1();
-          __syncthreads();
-        }
-        if constexpr (F::kMontgomery) {
-#pragma unroll
-          for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
-          if (q + 1 < nq) load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);
-        } else {
-#pragma unroll
-          for (int m = 0; m < E; ++m) v[m] = x[m];
-        }
-        typename Inv::Geo gq = g;
-        gq.hb = q;  // high block of the extended network (M31 per-block twiddles)
-        Fwd::template rounds<0>(ob, v, fwd_args(ai), tws_fwd, gq, tid);  // forward starts in round K-1's layout
-        if constexpr (!Net<F, true>::kGS) {
-#pragma unroll
-          for (int m = 0; m < E; ++m) v[m] = reduce2p<F>(v[m]);  // lazy CT values to [0, p)
-        }
-        Fwd::template st<0>(ob, v, tid);
-        tma::fence_proxy_async();
-        if (q == 0) {
-          if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-              atomicExch(ai.err, 1);
-              if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
-              tma::wait_all();
-            }
-            return;
-          }
-        } else {
-          __syncthreads();
-        }
+      if (!tile_body(cur, ostage, ai, tws_inv, tws_fwd, t, ok, mout, tid)) {
         if (tid == 0) {
-          tma::store_5d(mout, 0, g.s1, 0, (int32_t)q, g.s4, ob);
-          tma::commit();
+          atomicExch(ai.err, 1);
+          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          tma::wait_all();
         }
+        return;
       }
     }
     if (tid == 0) tma::wait_all();

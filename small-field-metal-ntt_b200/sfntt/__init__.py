@@ -139,6 +139,11 @@ class Context:
         _check(self.handle, _ffi.lib().sfntt_device_info(self.handle, buf, 256))
         return buf.value.decode()
 
+    def check_device_error(self) -> int:
+        """Status of the context's device error flag (SFNTT_TIMEOUT = 8 after a
+        bounded wait ran out in a _dev call or graph), without raising."""
+        return int(_ffi.lib().sfntt_check_device_error(self.handle))
+
     def launch_count(self) -> int:
         return int(_ffi.lib().sfntt_launch_count(self.handle))
 
@@ -590,6 +595,16 @@ class LdeBatch:
         h = ctypes.c_void_p()
         _check(self.ctx.handle, _ffi.lib().sfntt_batch_graph_create(self.ctx.handle, self.items, self.count, lanes,
                                                                     ctypes.byref(h)))
+        return Graph(h)
+
+    def persistent_graph(self, lanes: int = 8) -> "Graph":
+        """The batch with its eligible items (BabyBear / M31, 2^13..2^20
+        points, blow-up <= 16) in three persistent phase launches over a
+        device work list, the rest per item on `lanes` streams, in one graph
+        (sfntt_batch_persistent_create)."""
+        h = ctypes.c_void_p()
+        _check(self.ctx.handle, _ffi.lib().sfntt_batch_persistent_create(self.ctx.handle, self.items, self.count,
+                                                                         lanes, ctypes.byref(h)))
         return Graph(h)
 
 

@@ -60,6 +60,7 @@ SIGNATURES = {
     "sfntt_batch_prepare": (i32, [vp, vp, sz]),
     "sfntt_batch_run": (i32, [vp, vp, sz, vp]),
     "sfntt_batch_graph_create": (i32, [vp, vp, sz, i32, ctypes.POINTER(vp)]),
+    "sfntt_batch_persistent_create": (i32, [vp, vp, sz, i32, ctypes.POINTER(vp)]),
     "sfntt_graph_launch": (i32, [vp, vp]),
     "sfntt_graph_kernel_count": (u64, [vp]),
     "sfntt_graph_destroy": (None, [vp]),

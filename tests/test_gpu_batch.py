@@ -112,3 +112,59 @@ def test_tune_table_roundtrip(ctx, tmp_path):
     sfntt.tune_load(fresh, path)
     assert sfntt.LdeBatch(fresh, items).plan_of(0) == plan
     fresh.close()
+
+
+def test_persistent_phases_match_oracle(ctx):
+    """Items of both fields, 2^12..2^17 points, 1..40 columns, blow-ups
+    1/2/4/16: the eligible ones (2^13..2^20 points) run in the three
+    persistent phase launches over a device work list (BabyBear items with
+    >= 16 columns on staged twiddle chunks), the others per item beside them;
+    every output equals the oracle, on two replays of the graph."""
+    import torch
+    items = sfntt.uneven_workload(20, seed=31, log_n_range=(12, 17), cols_range=(1, 40))
+    items += [{"field": sfntt.FIELD_BABYBEAR, "log_n": 14, "batch": 17, "added_bits": 4},
+              {"field": sfntt.FIELD_M31, "log_n": 13, "batch": 33, "added_bits": 2},
+              {"field": sfntt.FIELD_BABYBEAR, "log_n": 13, "batch": 16, "added_bits": 0}]
+    bufs = _alloc(items, 4100)
+    batch = sfntt.LdeBatch(ctx, items)
+    batch.prepare()
+    g = batch.persistent_graph(lanes=4)
+    assert g.kernel_count() > 0
+    for rep in range(2):
+        for b in bufs:
+            b[2].zero_()
+        g.launch()
+        torch.cuda.synchronize()
+        assert ctx.check_device_error() == 0
+        for it, (x, _, d_out) in zip(items, bufs):
+            assert np.array_equal(d_out.cpu().numpy().view(np.uint32), _oracle(it, x)), (rep, it)
+    g.close()
+
+
+def test_persistent_phases_large_items(ctx):
+    """2^20-point items of both fields with many columns (the staged BabyBear
+    expansion and 12-layer contiguous passes): sampled columns against the
+    oracle and the whole output against the per-item launches."""
+    import torch
+    items = [{"field": sfntt.FIELD_BABYBEAR, "log_n": 20, "batch": 24, "added_bits": 1},
+             {"field": sfntt.FIELD_M31, "log_n": 19, "batch": 20, "added_bits": 2},
+             {"field": sfntt.FIELD_BABYBEAR, "log_n": 18, "batch": 5, "added_bits": 2}]
+    bufs = _alloc(items, 5100)
+    batch = sfntt.LdeBatch(ctx, items)
+    batch.prepare()
+    batch.run()
+    torch.cuda.synchronize()
+    plain = [b[2].clone() for b in bufs]
+    for b in bufs:
+        b[2].zero_()
+    g = batch.persistent_graph(lanes=2)
+    g.launch()
+    torch.cuda.synchronize()
+    for it, (x, _, d_out), ref in zip(items, bufs, plain):
+        assert torch.equal(d_out, ref), it
+        n, n_ext = 1 << it["log_n"], 1 << (it["log_n"] + it["added_bits"])
+        got = d_out.cpu().numpy().view(np.uint32)
+        for c in (0, it["batch"] - 1):
+            sub = dict(it, batch=1)
+            assert np.array_equal(got[c * n_ext:(c + 1) * n_ext], _oracle(sub, x[c * n:(c + 1) * n])), (it, c)
+    g.close()
