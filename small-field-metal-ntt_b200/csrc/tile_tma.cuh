@@ -382,6 +382,36 @@ struct TPass {
     return ((thread_tile_bits(k) >> sh) & mask) == 0u && ((RM<KD, P, LT, R, k>::cm(m) >> sh) & mask) == 0u;
   }
 
+  // Round k on two tiles' values at once, with one twiddle load per butterfly
+  // pair: the per-position twiddles tw[L][pos mod 2^L] of BabyBear / KoalaBear
+  // strided passes are the same for every high block, so the output blocks of
+  // one LDE expansion share them.
+  template <int k>
+  __device__ static __forceinline__ void round2(uint32_t (&va)[E], uint32_t (&vb)[E], const TmaArgs& a,
+                                                const uint2* tws, const Geo& g, uint32_t tid) {
+    static_assert(F::kMontgomery && KD == Kind::S, "twiddles shared across high blocks: per-position strided");
+    using M = RM<KD, P, LT, R, k>;
+    constexpr int r = Plan<P, R>::r(k);
+    constexpr int b = Plan<P, R>::b(k);
+    const uint32_t ct = M::ctid(tid);
+#pragma unroll
+    for (int jj = 0; jj < r; ++jj) {
+      const int j = DESC ? (r - 1 - jj) : jj;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        if (m & (1 << j)) continue;
+        if (unit_twiddle<k>(m, b + j)) {
+          butterfly_unit<F, DESC>(va[m], va[m | (1 << j)]);
+          butterfly_unit<F, DESC>(vb[m], vb[m | (1 << j)]);
+        } else {
+          const uint2 w = twiddle<k>(a, tws, g, ct, m, b + j);
+          butterfly<F, DESC>(va[m], va[m | (1 << j)], w);
+          butterfly<F, DESC>(vb[m], vb[m | (1 << j)], w);
+        }
+      }
+    }
+  }
+
   // ---- staging-buffer access in round k's layout ----
   template <int k>
   __device__ static constexpr bool vec() {
@@ -855,9 +885,19 @@ struct TExpand {
   // first store (the inverse and the first block touch only in-bounds shared
   // memory, twiddles and multipliers whatever the tile holds): then nothing is
   // stored and the result is false.
+  //
+  // BabyBear / KoalaBear with two or more output blocks run them in pairs
+  // (tile_body_pairs): blocks 2p and 2p+1 share their forward exchange, their
+  // pre-store barrier and every twiddle load of their second forward round.
+  // Requires the caller's thread 0 to have waited for the reads of every
+  // earlier store (cp.async.bulk.wait_group.read 0) before the tile's first
+  // barrier, since block 1 writes ostage without a barrier of its own.
   __device__ static __forceinline__ bool tile_body(uint32_t* cur, uint32_t* ostage, const TmaArgs& ai,
                                                    const uint2* tws_inv, const uint2* tws_fwd, uint32_t t, bool ok,
                                                    const CUtensorMap* mout, uint32_t tid) {
+    if constexpr (F::kMontgomery && K == 2) {
+      if (ai.log_q >= 1) return tile_body_pairs(cur, ostage, ai, tws_inv, tws_fwd, t, ok, mout, tid);
+    }
     using M = RM<Kind::S, P, LT, R, K - 1>;
     const uint32_t ct = M::ctid(tid);
     const uint32_t lo = ai.lo;
@@ -916,6 +956,62 @@ struct TExpand {
     return true;
   }
 
+  __device__ static __forceinline__ bool tile_body_pairs(uint32_t* cur, uint32_t* ostage, const TmaArgs& ai,
+                                                         const uint2* tws_inv, const uint2* tws_fwd, uint32_t t,
+                                                         bool ok, const CUtensorMap* mout, uint32_t tid) {
+    using M = RM<Kind::S, P, LT, R, K - 1>;
+    const uint32_t ct = M::ctid(tid);
+    const uint32_t lo = ai.lo;
+    const uint32_t n = 1u << ai.log_n;
+    const uint32_t nq = 1u << ai.log_q;
+    const typename Inv::Geo g = Inv::geo(ai, t);
+    const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
+    const FwdArgs af = fwd_args(ai);
+    uint32_t x[E];
+    uint2 w[E];
+    load_mul(w, ai.mul + pos_t, lo);  // block 0's multipliers, in flight during the inverse layers
+    Inv::template ld<0>(cur, x, tid);
+    Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
+    for (uint32_t q = 0; q < nq; q += 2) {
+      // blocks q (from cur) and q+1 (from ostage): the stores that last read
+      // them are the previous pair's (for q = 0 the previous tile's, whose
+      // reads thread 0 waited for before the inverse layers' barrier)
+      if (q >= 2) {
+        load_mul(w, ai.mul + (uint64_t)q * n + pos_t, lo);  // (4x and up: not prefetched, to save registers)
+        if (tid == 0) tma::wait_reads();
+        __syncthreads();
+      }
+      uint32_t va[E], vb[E];
+#pragma unroll
+      for (int m = 0; m < E; ++m) va[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
+      load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);  // in flight during block q's first round
+      Fwd::template round<K - 1>(va, af, tws_fwd, g, tid);
+#pragma unroll
+      for (int m = 0; m < E; ++m) vb[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
+      Fwd::template round<K - 1>(vb, af, tws_fwd, g, tid);
+      Fwd::template st<K - 1>(cur, va, tid);
+      Fwd::template st<K - 1>(ostage, vb, tid);
+      __syncthreads();  // the exchange of both blocks (strided tiles exchange across the CTA)
+      Fwd::template ld<0>(cur, va, tid);
+      Fwd::template ld<0>(ostage, vb, tid);
+      Fwd::template round2<0>(va, vb, af, tws_fwd, g, tid);
+      Fwd::template st<0>(cur, va, tid);
+      Fwd::template st<0>(ostage, vb, tid);
+      tma::fence_proxy_async();
+      if (q == 0) {
+        if (__syncthreads_or(!ok)) return false;
+      } else {
+        __syncthreads();
+      }
+      if (tid == 0) {
+        tma::store_5d(mout, 0, g.s1, 0, (int32_t)q, g.s4, cur);
+        tma::store_5d(mout, 0, g.s1, 0, (int32_t)q + 1, g.s4, ostage);
+        tma::commit();
+      }
+    }
+    return true;
+  }
+
   __device__ static void run(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
@@ -960,10 +1056,12 @@ struct TExpand {
       const uint32_t buf = it & 1u;
       uint32_t* cur = stage + buf * TWORDS;
       const uint32_t tn = t + t_step;
-      if (tid == 0 && tn < t_end) {
-        tma::wait_reads();
-        tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
-        Inv::tma_load(min, Inv::geo(ai, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+      if (tid == 0) {
+        tma::wait_reads();  // every earlier store has read its buffer (tile_body relies on it)
+        if (tn < t_end) {
+          tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
+          Inv::tma_load(min, Inv::geo(ai, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+        }
       }
       if constexpr (LSTAGE) {
         // Every thread passed the previous tile's last barrier after its last

@@ -201,9 +201,9 @@ worklist_x_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
     uint32_t* cur = stage + buf * TW;
     bool issued = false;
     if (tid == 0) {
+      tma::wait_reads();  // every earlier store has read its buffer (the expansion's tile step relies on it)
       uint32_t ni, nt;
       if (next_tile(cursor, units, n_units, counter, ni, nt)) {
-        tma::wait_reads();
         const WorkItem& wn = items[ni];
         tma::mbar_expect_tx(&bar[buf ^ 1u], kTileBytes);
         G::tma_load(&wn.min, G::geo(wn.a, nt), stage + (buf ^ 1u) * TW, &bar[buf ^ 1u]);
