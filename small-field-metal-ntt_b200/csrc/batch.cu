@@ -143,8 +143,9 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
           uint32_t plo[4], pcnt[4];
           const int k = tma_split(0, lo, plo, pcnt, c12);
           for (int i = 1; i < k; ++i) {
-            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], true, s, &t));
-            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], false, s, &t));
+            const bool compact = twist_compact_for(plo[i], pcnt[i]);
+            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], true, s, &t, compact));
+            SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], false, s, &t, compact));
           }
         }
       }

@@ -174,8 +174,11 @@ Status monty_natural_tables(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t 
 
 // Twist of a strided BabyBear / KoalaBear pass over layers [lo, lo + P),
 // indexed by column position mod 2^(lo+P) (cached like the LDE tables).
+// compact: one word per entry, the Shoup companion w' (w = mulhi(w', p) + 1),
+// for twists spanning 2^22 positions or more (the pair table would be 32 MiB+).
 Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream,
-                         const uint2** out);
+                         const uint2** out, bool compact = false);
+inline bool twist_compact_for(uint32_t lo, uint32_t P) { return lo + P >= 22; }
 
 // Kernel drivers (ntt.cu / lde.cu / elementwise.cu)
 Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d_data, uint32_t log_n,

@@ -110,7 +110,8 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
         }
         if (!plain) continue;
         const int nb = pi + 1;  // the strided chunk just above pi
-        SFNTT_TRY(monty_twist_table(ctx, field, lo[nb], cnt[nb], inverse, s, &req[i].twist));
+        req[i].twist_compact = twist_compact_for(lo[nb], cnt[nb]);
+        SFNTT_TRY(monty_twist_table(ctx, field, lo[nb], cnt[nb], inverse, s, &req[i].twist, req[i].twist_compact));
         req[i].twist_mask = (1u << (lo[nb] + cnt[nb])) - 1u;
       }
     }

@@ -49,6 +49,10 @@ struct TmaArgs {
   // twist[pos & twist_mask]; nullptr = none
   const uint2* twist;
   uint32_t twist_mask;
+  // twist_compact: `twist` holds one word per entry, the Shoup companion w' of
+  // the twist w, which gives back w = mulhi(w', p) + 1 (w' = floor(w 2^32 / p)
+  // and w != 0): half the bytes, for tables that would not stay in L2
+  uint32_t twist_compact;
   // M31 contiguous passes: the table's copy of layers 0..3 in first-round
   // order (entry n of an M31 table with n >= 2^13; see round0_permute_kernel);
   // nullptr = read the layers from the table itself
@@ -560,10 +564,19 @@ struct TPass {
   __device__ static __forceinline__ void twist(uint32_t (&v)[E], const TmaArgs& a, const Geo& g, uint32_t tid) {
     using M = RM<KD, P, LT, R, k>;
     const uint32_t ct = M::ctid(tid);
+    if (a.twist_compact) {
+      const uint32_t* tc = reinterpret_cast<const uint32_t*>(a.twist);
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      const uint2 w = __ldg(a.twist + (pos_of<k>(a, g, ct, m) & a.twist_mask));
-      v[m] = mul_shoup<F>(v[m], w.x, w.y);
+      for (int m = 0; m < E; ++m) {
+        const uint32_t ws = __ldg(tc + (pos_of<k>(a, g, ct, m) & a.twist_mask));
+        v[m] = mul_shoup<F>(v[m], __umulhi(ws, F::P) + 1u, ws);
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const uint2 w = __ldg(a.twist + (pos_of<k>(a, g, ct, m) & a.twist_mask));
+        v[m] = mul_shoup<F>(v[m], w.x, w.y);
+      }
     }
   }
 

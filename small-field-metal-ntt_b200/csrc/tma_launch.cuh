@@ -23,6 +23,7 @@ struct TmaRequest {
   uint32_t scale_w;  // canonical multiplier for the outputs; 0 = none
   const uint2* twist = nullptr;  // BabyBear four-step twist at the boundary
   uint32_t twist_mask = 0;
+  bool twist_compact = false;    // the twist table holds Shoup companions only (TmaArgs::twist_compact)
   bool plain = false;            // BabyBear strided pass: plain sub-transform (twist by neighbours)
   // per-position twiddles staged in shared memory, one CTA per SM walking the
   // columns (BabyBear 8-layer strided or M31 12-layer contiguous passes, n >= 2^13)
@@ -101,6 +102,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   a.scale_ws = (uint32_t)(((uint64_t)r.scale_w << 32) / F::P);
   a.twist = r.twist;
   a.twist_mask = r.twist_mask;
+  a.twist_compact = r.twist_compact ? 1u : 0u;
   if constexpr (KD == Kind::C) {
     const uint32_t rows = HALVES ? T::HROWS : kTileWords / 32;
     SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch, rows));

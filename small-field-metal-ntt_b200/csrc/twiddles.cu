@@ -144,7 +144,7 @@ __global__ void power_table_kernel(uint2* tab, uint32_t log_len, uint32_t count,
 // followed by this factor, and its DIT layers equal the plain sub-DIT applied
 // to inputs multiplied by the inverse factor.
 template <class F>
-__global__ void twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_monty) {
+__global__ void twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_monty, int compact) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (1u << (lo + P))) return;
   const uint32_t l = t & ((1u << lo) - 1u);
@@ -152,7 +152,8 @@ __global__ void twist_kernel(uint2* tab, uint32_t lo, uint32_t P, uint32_t g_mon
   const uint32_t re = __brev(e) >> (32u - P);
   uint32_t w = pow_var<F>(g_monty, l * re);
   w = to_canonical(F{}, w);
-  tab[t] = make_uint2(w, shoup_of<F>(w));
+  if (compact) reinterpret_cast<uint32_t*>(tab)[t] = shoup_of<F>(w);  // w = mulhi(w', p) + 1
+  else tab[t] = make_uint2(w, shoup_of<F>(w));
 }
 
 // Natural-order LDE multipliers M_r[i] = n^-1 base_r^rev(i), stored in the
@@ -388,10 +389,10 @@ Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added
 namespace sfntt {
 
 Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, bool inverse, cudaStream_t stream,
-                         const uint2** out) {
+                         const uint2** out, bool compact) {
   const host::MontyField& f = host::monty_field(field);
   if (lo + P > f.two_adicity || P == 0 || P > 8) return {SFNTT_INVALID_ARGUMENT, "twist span"};
-  const auto key = std::make_tuple(monty_slot(field), lo, P, inverse ? 1u : 0u, 2);
+  const auto key = std::make_tuple(monty_slot(field), lo, P, inverse ? 1u : 0u, compact ? 3 : 2);
   auto it = ctx->lde_tabs.find(key);
   if (it == ctx->lde_tabs.end()) {
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twist table not prepared before capture"};
@@ -399,10 +400,11 @@ Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, boo
     if (inverse) g = host::invmod(g, f.p);
     const uint32_t count = 1u << (lo + P);
     DevBuf buf;
-    SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
+    SFNTT_TRY(buf.reserve((size_t)count * (compact ? sizeof(uint32_t) : sizeof(uint2))));
     with_monty(field, [&](auto fld) {
       using F = decltype(fld);
-      twist_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), lo, P, host::to_monty(f, g));
+      twist_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), lo, P, host::to_monty(f, g),
+                                                                 compact ? 1 : 0);
       return 0;
     });
     Status s = sync_after_build(ctx, stream, "twist_kernel");
