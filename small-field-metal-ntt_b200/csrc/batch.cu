@@ -128,7 +128,10 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
     if (ext + 1 > adicity) return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(adicity - 1)};
     if (it.log_n) SFNTT_TRY(monty_twiddles(ctx, f, true, it.log_n, s, &t));
     if (ext) SFNTT_TRY(monty_twiddles(ctx, f, false, ext, s, &t));
-    if (it.added_bits <= 4) SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 0, s, &t));
+    if (it.added_bits <= 4) {
+      SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 0, s, &t));
+      if (it.log_n >= 13) SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 2, s, &t));
+    }
     SFNTT_TRY(monty_lde_table(ctx, f, it.log_n, it.added_bits, it.shift_monty, 1, s, &t));
     if (it.log_n >= 13) {
       SFNTT_TRY(monty_twist_table(ctx, f, it.log_n - 8, 8, true, s, &t));

@@ -491,6 +491,8 @@ int sfntt_prepare_lde(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_
       if (log_n) s = sfntt::monty_twiddles(ctx, field, true, log_n, st, &tw);
       if (s.ok()) s = sfntt::monty_twiddles(ctx, field, false, log_n + added_bits, st, &tw);
       if (s.ok() && added_bits <= 4) s = sfntt::monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 0, st, &tw);
+      if (s.ok() && added_bits <= 4 && log_n >= 13)
+        s = sfntt::monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 2, st, &tw);
       if (s.ok()) s = sfntt::monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 1, st, &tw);
       // the natural-order 2x route's tables (its scratch depends on the batch and is reserved on first use)
       if (s.ok() && added_bits == 1 && log_n >= 13 && log_n <= 20) {

@@ -162,6 +162,8 @@ Status m31_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t s
 Status m31_circle_twiddles(sfntt_ctx* ctx, bool inverse, uint32_t log_n, cudaStream_t stream, const uint2** out);
 // kind 0: fused LDE multipliers M_q[i] = n^-1 (shift g^{rev(q)})^i, q < 2^added, i < n
 // kind 1: plain shift powers shift^i, i < n_ext (unfused path)
+// kind 2: kind 0 in the TMA expansion's tile order (log_n >= 13): entry
+//         q n + (chunk 2^13 + e 32 + u) is M_q[chunk 32 + u + e 2^(log_n - 8)]
 Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added_bits, uint32_t shift_monty,
                        int kind, cudaStream_t stream, const uint2** out);
 

@@ -308,8 +308,9 @@ Status monty_lde_rows(sfntt_ctx* ctx, const uint32_t* d_in, uint64_t in_stride, 
     const uint2 *tw_inv = nullptr, *tw_fwd = nullptr, *mul = nullptr;
     SFNTT_TRY(monty_twiddles(ctx, field, true, log_n, s, &tw_inv));
     SFNTT_TRY(monty_twiddles(ctx, field, false, log_ext, s, &tw_fwd));
-    SFNTT_TRY(monty_lde_table(ctx, field, log_n, added_bits, shift_monty, 0, s, &mul));
     const bool tma_ok = !ctx->no_tma && log_n >= 13 && aligned16(d_in) && aligned16(d_out);
+    // the TMA expansion reads its multipliers in tile order (kind 2)
+    SFNTT_TRY(monty_lde_table(ctx, field, log_n, added_bits, shift_monty, tma_ok ? 2 : 0, s, &mul));
     if (tma_ok) {
       // I1: inverse layers [0, lo) into the output buffer, ending with the
       // four-step pre-twist of the expand's sub-iDFT; X: the persistent TMA

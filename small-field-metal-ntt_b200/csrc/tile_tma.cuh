@@ -878,11 +878,15 @@ struct TExpand {
   // one block ahead and stage twiddles, one CTA per SM.
   static constexpr int kCtasPerSm = F::kMontgomery ? 1 : 2;
 
-  // Multipliers M_q of the thread's 16 slots (round K-1 layout) from mq = M_q + pos_t.
-  __device__ static __forceinline__ void load_mul(uint2 (&w)[E], const uint2* mq, uint32_t lo) {
+  // Multipliers M_q of the thread's 16 slots (round K-1 layout).  The table is
+  // in tile order (kind 2: entry q n + chunk 2^13 + c for tile word c of the
+  // chunk's tiles), so from mq = table + q n + chunk 2^13 + ctid every slot is
+  // a compile-time offset (its tile bits), and each slot's load is a
+  // contiguous 256-byte run across a warp.
+  __device__ static __forceinline__ void load_mul(uint2 (&w)[E], const uint2* mq) {
     using M = RM<Kind::S, P, LT, R, K - 1>;
 #pragma unroll
-    for (int m = 0; m < E; ++m) w[m] = __ldg(mq + (M::cm(m) & 31u) + ((M::cm(m) >> 5) << lo));
+    for (int m = 0; m < E; ++m) w[m] = __ldg(mq + M::cm(m));
   }
 
   // LSTAGE: the 32-position chunk of tile t, whose per-position twiddles the
@@ -913,17 +917,15 @@ struct TExpand {
     }
     using M = RM<Kind::S, P, LT, R, K - 1>;
     const uint32_t ct = M::ctid(tid);
-    const uint32_t lo = ai.lo;
     const uint32_t n = 1u << ai.log_n;
     const uint32_t nq = 1u << ai.log_q;
     uint32_t x[E], v[E];
     const typename Inv::Geo g = Inv::geo(ai, t);
-    // position of slot m: pos_base + u + (e << lo)
-    const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
+    const uint2* mt = ai.mul + ((uint32_t)g.s1 << kTileBits) + ct;  // this thread's multipliers of block 0
     // BabyBear multipliers are software-pipelined: block q+1's are loaded
     // while block q's forward layers run (block 0's during the inverse).
     uint2 w[F::kMontgomery ? E : 1];
-    if constexpr (F::kMontgomery) load_mul(w, ai.mul + pos_t, lo);
+    if constexpr (F::kMontgomery) load_mul(w, mt);
     Inv::template ld<0>(cur, x, tid);
     Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
     if constexpr (!F::kMontgomery) {
@@ -942,7 +944,7 @@ struct TExpand {
       if constexpr (F::kMontgomery) {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
-        if (q + 1 < nq) load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);
+        if (q + 1 < nq) load_mul(w, mt + (uint64_t)(q + 1) * n);
       } else {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = x[m];
@@ -974,15 +976,14 @@ struct TExpand {
                                                          bool ok, const CUtensorMap* mout, uint32_t tid) {
     using M = RM<Kind::S, P, LT, R, K - 1>;
     const uint32_t ct = M::ctid(tid);
-    const uint32_t lo = ai.lo;
     const uint32_t n = 1u << ai.log_n;
     const uint32_t nq = 1u << ai.log_q;
     const typename Inv::Geo g = Inv::geo(ai, t);
-    const uint32_t pos_t = g.pos_base + (ct & 31u) + ((ct >> 5) << lo);
+    const uint2* mt = ai.mul + ((uint32_t)g.s1 << kTileBits) + ct;  // this thread's multipliers of block 0
     const FwdArgs af = fwd_args(ai);
     uint32_t x[E];
     uint2 w[E];
-    load_mul(w, ai.mul + pos_t, lo);  // block 0's multipliers, in flight during the inverse layers
+    load_mul(w, mt);  // block 0's multipliers, in flight during the inverse layers
     Inv::template ld<0>(cur, x, tid);
     Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
     for (uint32_t q = 0; q < nq; q += 2) {
@@ -990,14 +991,14 @@ struct TExpand {
       // them are the previous pair's (for q = 0 the previous tile's, whose
       // reads thread 0 waited for before the inverse layers' barrier)
       if (q >= 2) {
-        load_mul(w, ai.mul + (uint64_t)q * n + pos_t, lo);  // (4x and up: not prefetched, to save registers)
+        load_mul(w, mt + (uint64_t)q * n);  // (4x and up: not prefetched, to save registers)
         if (tid == 0) tma::wait_reads();
         __syncthreads();
       }
       uint32_t va[E], vb[E];
 #pragma unroll
       for (int m = 0; m < E; ++m) va[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
-      load_mul(w, ai.mul + (uint64_t)(q + 1) * n + pos_t, lo);  // in flight during block q's first round
+      load_mul(w, mt + (uint64_t)(q + 1) * n);  // in flight during block q's first round
       Fwd::template round<K - 1>(va, af, tws_fwd, g, tid);
 #pragma unroll
       for (int m = 0; m < E; ++m) vb[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);

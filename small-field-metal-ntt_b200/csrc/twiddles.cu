@@ -124,14 +124,19 @@ __global__ void round0_permute_kernel(uint2* tab, uint32_t log_n) {
 
 struct LdeBases { uint32_t b[16]; };
 
-// kind 0: tab[q*n + i] = n^-1 * base_q^i ; kind 1: tab[i] = base_0^i
+// kind 0: tab[q*n + i] = n^-1 * base_q^i ; kind 1: tab[i] = base_0^i ;
+// kind 2 (tile_lo = log n - 8 > 0): kind 0's entries in the order of the TMA
+// expansion's strided tiles -- entry q*n + (chunk 2^13 + e 32 + u) holds
+// position i = chunk 32 + u + e 2^tile_lo -- so a thread's multipliers sit at
+// compile-time offsets from one base.
 template <class F>
 __global__ void power_table_kernel(uint2* tab, uint32_t log_len, uint32_t count, LdeBases bases,
-                                   uint32_t scale_monty) {
+                                   uint32_t scale_monty, uint32_t tile_lo) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
   const uint32_t q = t >> log_len;
-  const uint32_t i = t & ((1u << log_len) - 1u);
+  uint32_t i = t & ((1u << log_len) - 1u);
+  if (tile_lo) i = ((i >> 13) << 5) + (i & 31u) + (((i >> 5) & 255u) << tile_lo);
   uint32_t w = pow_var<F>(bases.b[q], i);
   w = mul_var<F>(w, scale_monty);
   w = to_canonical(F{}, w);
@@ -343,7 +348,7 @@ Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added
   if (!ext_fits(log_n, added_bits, f.two_adicity - 1))
     return {SFNTT_INVALID_SIZE, "log_n + added_bits must be <= " + std::to_string(f.two_adicity - 1)};
   const uint32_t log_ext = log_n + added_bits;
-  if (kind == 0 && added_bits > 4) return {SFNTT_INVALID_ARGUMENT, "fused LDE supports added_bits <= 4"};
+  if (kind != 1 && added_bits > 4) return {SFNTT_INVALID_ARGUMENT, "fused LDE supports added_bits <= 4"};
   const auto key = std::make_tuple(monty_slot(field), log_n, added_bits, shift_monty, kind);
   auto it = ctx->lde_tabs.find(key);
   if (it == ctx->lde_tabs.end()) {
@@ -351,7 +356,8 @@ Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added
     const uint32_t shift = shift_monty ? host::from_monty(f, shift_monty) : host::two_adic_generator(f, log_ext + 1);
     LdeBases B{};
     uint32_t log_len, count, scale;
-    if (kind == 0) {
+    if (kind == 2 && log_n < 13) return {SFNTT_INVALID_ARGUMENT, "tile-ordered multipliers need log_n >= 13"};
+    if (kind == 0 || kind == 2) {
       // quarter q of the zero-padded DIF gets g_ext^{i * rev(q)} from its top
       // added_bits layers; fold it with the shift and n^-1 into one multiplier
       const uint32_t g_ext = host::two_adic_generator(f, log_ext);
@@ -373,7 +379,8 @@ Status monty_lde_table(sfntt_ctx* ctx, int field, uint32_t log_n, uint32_t added
     SFNTT_TRY(buf.reserve((size_t)count * sizeof(uint2)));
     with_monty(field, [&](auto fld) {
       using F = decltype(fld);
-      power_table_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_len, count, B, scale);
+      power_table_kernel<F><<<(count + 255) / 256, 256, 0, stream>>>(buf.as<uint2>(), log_len, count, B, scale,
+                                                                       kind == 2 ? log_n - 8 : 0u);
       return 0;
     });
     Status s = sync_after_build(ctx, stream, "power_table_kernel");
@@ -392,7 +399,7 @@ Status monty_twist_table(sfntt_ctx* ctx, int field, uint32_t lo, uint32_t P, boo
                          const uint2** out, bool compact) {
   const host::MontyField& f = host::monty_field(field);
   if (lo + P > f.two_adicity || P == 0 || P > 8) return {SFNTT_INVALID_ARGUMENT, "twist span"};
-  const auto key = std::make_tuple(monty_slot(field), lo, P, inverse ? 1u : 0u, compact ? 3 : 2);
+  const auto key = std::make_tuple(monty_slot(field), lo, P, inverse ? 1u : 0u, compact ? 5 : 2);
   auto it = ctx->lde_tabs.find(key);
   if (it == ctx->lde_tabs.end()) {
     if (capturing(stream)) return {SFNTT_INVALID_ARGUMENT, "twist table not prepared before capture"};

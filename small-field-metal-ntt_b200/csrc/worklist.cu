@@ -154,17 +154,17 @@ worklist_c_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
 
 // ------------------------------------------------------------------ phase 2 --
 using XBbStaged = TExpand<BabyBear, 8, false, true>;
-using XBb = TExpand<BabyBear, 8, false, false>;
 using XM31 = TExpand<M31, 8, false, false>;
 static_assert(XBbStaged::TW_ENTRIES == XBbStaged::Inv::LCHUNK_ENTRIES, "staged chunk per direction");
 
-// Expansions of every item (strided 8-layer tiles).  BabyBear items with many
-// columns read their per-position twiddles from a staged 32-position chunk
-// (restaged when the item or the chunk changes), the others from L2.
+// Expansions of every item (strided 8-layer tiles).  BabyBear items read their
+// per-position twiddles from a staged 32-position chunk (restaged when the item
+// or the chunk changes; units keep a chunk's columns together); M31 twiddles
+// are uniform across a tile's lanes and come from L2.
 __global__ void __launch_bounds__(512, 1)
 worklist_x_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict__ units, uint32_t n_units,
                   uint32_t* counter) {
-  using G = XBb::Inv;  // strided tile geometry and TMA (field-independent)
+  using G = XM31::Inv;  // strided tile geometry and TMA (field-independent)
   constexpr uint32_t TW = kTileWords;
   extern __shared__ __align__(1024) uint32_t smem_words[];
   uint32_t* stage = smem_words;
@@ -230,8 +230,7 @@ worklist_x_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
     const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
     bool good;
     if (w.field == SFNTT_BABYBEAR) {
-      good = w.lstage ? XBbStaged::tile_body(cur, ostage, w.a, tws_inv, tws_fwd, t, ok, &w.mout, tid)
-                      : XBb::tile_body(cur, ostage, w.a, tws_inv, tws_fwd, t, ok, &w.mout, tid);
+      good = XBbStaged::tile_body(cur, ostage, w.a, tws_inv, tws_fwd, t, ok, &w.mout, tid);
     } else {
       good = XM31::tile_body(cur, ostage, w.a, tws_inv, tws_fwd, t, ok, &w.mout, tid);
     }
@@ -319,12 +318,13 @@ Status worklist_add(sfntt_ctx* ctx, WorkPhase& ph, int phase, const sfntt_lde_it
     a.log_q = it.added_bits;
     if (bb) {
       const uint2* mul = nullptr;
-      SFNTT_TRY(monty_lde_table(ctx, it.field, log_n, it.added_bits, it.shift_monty, 0, s, &mul));
+      SFNTT_TRY(monty_lde_table(ctx, it.field, log_n, it.added_bits, it.shift_monty, 2, s, &mul));
       a.mul = mul;
-      // the chunk's twiddles are reused across >= 16 columns (lde.cu's rule):
-      // a unit is one chunk's tiles of up to 32 columns
-      w.lstage = it.batch >= 16 ? 1u : 0u;
-      if (w.lstage) {
+      // BabyBear expansions read their per-position twiddles from a staged
+      // 32-position chunk (restaged when the item or chunk changes): a unit
+      // is one chunk's tiles of up to 32 columns
+      w.lstage = 1u;
+      {
         const uint32_t chunks = 1u << (lo - 5);
         const uint32_t cols_per = std::min<uint32_t>(it.batch, 32u);
         for (uint32_t c = 0; c < chunks; ++c)
