@@ -129,7 +129,7 @@ struct sfntt_ctx {
   int tma_ctas = 0;
   // contiguous 8- and 12-layer TMA passes run their two CTA halves as
   // independent pipelines (half tiles, own barriers); off: whole tiles
-  bool c_halves = false;
+  bool c_halves = true;
   // autotuned plans: "field/log_n/columns/added_bits" -> sfntt_plan
   std::map<std::string, int> tuned;
 
