@@ -875,8 +875,11 @@ struct TExpand {
   static_assert(F::kMontgomery || !PLAIN, "M31 passes have no plain variant");
   // M31 stages no twiddles (3 x 32 KiB of shared memory) and fits 64 registers:
   // two CTAs per SM; BabyBear / KoalaBear keep their multipliers in registers
-  // one block ahead and stage twiddles, one CTA per SM.
-  static constexpr int kCtasPerSm = F::kMontgomery ? 1 : 2;
+  // one block ahead and stage per-position twiddles, one CTA per SM.  The
+  // four-step (PLAIN) form stages only the 2 x 255 lane-independent twiddles
+  // and loads each multiplier where it is used, so it too fits 64 registers
+  // and two CTAs per SM.
+  static constexpr int kCtasPerSm = (F::kMontgomery && !PLAIN) ? 1 : 2;
 
   // Multipliers M_q of the thread's 16 slots (round K-1 layout).  The table is
   // in tile order (kind 2: entry q n + chunk 2^13 + c for tile word c of the
@@ -912,7 +915,7 @@ struct TExpand {
   __device__ static __forceinline__ bool tile_body(uint32_t* cur, uint32_t* ostage, const TmaArgs& ai,
                                                    const uint2* tws_inv, const uint2* tws_fwd, uint32_t t, bool ok,
                                                    const CUtensorMap* mout, uint32_t tid) {
-    if constexpr (F::kMontgomery && K == 2) {
+    if constexpr (F::kMontgomery && K == 2 && !PLAIN) {
       if (ai.log_q >= 1) return tile_body_pairs(cur, ostage, ai, tws_inv, tws_fwd, t, ok, mout, tid);
     }
     using M = RM<Kind::S, P, LT, R, K - 1>;
@@ -923,9 +926,11 @@ struct TExpand {
     const typename Inv::Geo g = Inv::geo(ai, t);
     const uint2* mt = ai.mul + ((uint32_t)g.s1 << kTileBits) + ct;  // this thread's multipliers of block 0
     // BabyBear multipliers are software-pipelined: block q+1's are loaded
-    // while block q's forward layers run (block 0's during the inverse).
-    uint2 w[F::kMontgomery ? E : 1];
-    if constexpr (F::kMontgomery) load_mul(w, mt);
+    // while block q's forward layers run (block 0's during the inverse); the
+    // four-step form loads them where they are used (registers for 2 CTAs).
+    constexpr bool kPrefetch = F::kMontgomery && !PLAIN;
+    uint2 w[kPrefetch ? E : 1];
+    if constexpr (kPrefetch) load_mul(w, mt);
     Inv::template ld<0>(cur, x, tid);
     Inv::template rounds<0>(cur, x, ai, tws_inv, g, tid);  // x: round K-1 layout
     if constexpr (!F::kMontgomery) {
@@ -941,10 +946,18 @@ struct TExpand {
         if (tid == 0) tma::wait_reads_1();
         __syncthreads();
       }
-      if constexpr (F::kMontgomery) {
+      if constexpr (kPrefetch) {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = mul_shoup<F>(x[m], w[m].x, w[m].y);
         if (q + 1 < nq) load_mul(w, mt + (uint64_t)(q + 1) * n);
+      } else if constexpr (F::kMontgomery) {
+        using MK = RM<Kind::S, P, LT, R, K - 1>;
+        const uint2* mq = mt + (uint64_t)q * n;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const uint2 wm = __ldg(mq + MK::cm(m));
+          v[m] = mul_shoup<F>(x[m], wm.x, wm.y);
+        }
       } else {
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = x[m];
