@@ -324,8 +324,8 @@ size_t sfntt_server_pending(const sfntt_server *server);
  * and this applies it across requests): when the request at the front of the
  * queue launches, up to max_requests - 1 queued requests of the same field,
  * log_n, added_bits, shift and plan that each leave part of the GPU idle join
- * it as further columns of one batch, as long as the launch fits the GPU's
- * free width.  Their inputs are gathered into one arena block (device
+ * it as further columns of one batch (the front request alone decides
+ * admission).  Their inputs are gathered into one arena block (device
  * requests: a device-to-device copy from d_in), one LDE runs over all the
  * columns, and each request's output is its slice of the launch's output.
  * max_requests = 1 (the default) launches every request alone. */

@@ -158,9 +158,8 @@ bool same_shape(const sfntt_lde_item& a, const sfntt_lde_item& b) {
 
 // Admits queued requests in order while a slot is free, the GPU has room and
 // the arena has room.  The request at the front of the queue launches; with
-// packing on, queued requests of its shape (up to max_pack, and while the
-// launch stays within the GPU's free width) join it as further columns of
-// the same batch: their inputs are gathered into one arena block (host
+// packing on, queued requests of its shape (up to max_pack) join it as
+// further columns of the same batch: their inputs are gathered into one arena block (host
 // requests copy there from the host, device requests from d_in), one LDE runs
 // over all the columns, and each request's output is its slice of the
 // launch's output block (copied back to the host for host requests).
@@ -178,12 +177,13 @@ Status admit(sfntt_server* sv) {
     std::vector<size_t> members{0};
     uint32_t cols = front.item.batch;
     if (sv->max_pack > 1 && packable(front)) {
+      // Same-shape requests join until max_pack: one launch of their columns
+      // never takes longer than their launches one after another, so the
+      // launch may be wider than the GPU's free width (it then runs as
+      // running work drains); the front request alone decided admission.
       for (size_t q = 1; q < sv->queue.size() && (int)members.size() < sv->max_pack; ++q) {
         const Request& c = sv->queue[q];
         if (!packable(c) || !same_shape(c.item, front.item)) continue;
-        sfntt_lde_item probe = front.item;
-        probe.batch = cols + c.item.batch;
-        if (width_of(sv, probe) > room + 1e-9) break;
         members.push_back(q);
         cols += c.item.batch;
       }
@@ -229,7 +229,7 @@ Status admit(sfntt_server* sv) {
     Group& g = sv->groups[gid];
     g.off = off;
     g.refs = (int)members.size();
-    g.width = width_of(sv, it);
+    g.width = std::min(std::max(width_of(sv, it), front.width), std::max(room, front.width));
     g.exclusive = exclusive(it);
     sv->slot_group[slot] = gid;
     sv->exclusive_running = g.exclusive;
