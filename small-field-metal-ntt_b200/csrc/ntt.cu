@@ -88,9 +88,9 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
       r.contiguous = lo[pi] == 0;
       r.batch = batch;
       r.scale_w = (i == kt - 1) ? scale_w : 0u;
-      // M31 12-layer contiguous passes over many columns: a tile's twiddles
-      // (twice its own size) are staged once for all of its columns
-      r.lstage = !is_monty(field) && r.contiguous && r.P == 12 && log_n >= 13 && batch >= 16;
+      // M31 contiguous passes over many columns: a tile's per-block twiddles
+      // (twice its own size in L2 reads) are staged once for all its columns
+      r.lstage = !is_monty(field) && r.contiguous && log_n >= 13 && batch >= 16;
       ok = tma_pass_ok(r);
     }
     if (ok && is_monty(field)) {

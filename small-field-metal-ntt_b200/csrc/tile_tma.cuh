@@ -98,11 +98,11 @@ struct TPass {
   // twiddles in shared memory.  BabyBear strided tiles: the per-position
   // twiddles of a 32-position chunk (the staged lookup takes the lane part of
   // a position from the thread alone: with P = 8 every slot bit of both rounds
-  // is a layer bit above the lanes).  M31 12-layer contiguous tiles: the
-  // per-block twiddles of the tile's 2^13 positions.
+  // is a layer bit above the lanes).  M31 contiguous tiles (any layer
+  // count): the per-block twiddles of the tile's 2^13 positions.
   static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN && P == 8) ||
-                    (KD == Kind::C && !F::kMontgomery && P == 12 && !TW),
-                "position staging: BabyBear 8-layer strided or M31 12-layer contiguous tiles");
+                    (KD == Kind::C && !F::kMontgomery && !TW),
+                "position staging: BabyBear 8-layer strided or M31 contiguous tiles");
   static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
   static constexpr int CB = P + LT;
   static constexpr int R = 4;
@@ -203,15 +203,20 @@ struct TPass {
            mp.ngrp == 1 && mp.gshift[0] == 4 && mp.gmask[0] == (1u << (kTileBits - 4)) - 1u;
   }
   static constexpr bool kRound0Copy = !F::kMontgomery && KD == Kind::C && round0_linear();
-  static_assert(!LSTAGE || KD == Kind::S || kRound0Copy, "M31 tile staging starts from the first-round copy");
+  // M31 12-layer staging keeps layers 0..3 in the first round's thread order
+  // (from the table's first-round copy); other layer counts stage every layer
+  // in table order.
+  static constexpr bool kStageThreadOrder = LSTAGE && KD == Kind::C && P == 12;
+  static_assert(!kStageThreadOrder || kRound0Copy, "M31 tile staging starts from the first-round copy");
   static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
   // M31 tile staging: the twiddles of a tile's 2^13 positions, one word each
   // -- the Shoup companion w' = floor(w 2^32 / p), which for the Mersenne
   // prime (2^32 / p = 2 + 2 / p) is 2w + (w >= 2^30), so w = w' >> 1, one
   // shift -- laid out like a
-  // 2^13-point table with layer L at 8192 - (8192 >> L); layers 0..3 (words
-  // [0, 7680)) are ordered by thread: layer j gives thread t its 2^(3-j)
-  // twiddles as vectors of v = min(2^(3-j), 4) words at v (g NT + t), group g.
+  // 2^13-point table with layer L at 8192 - (8192 >> L); with 12 layers,
+  // layers 0..3 (words [0, 7680)) are ordered by thread: layer j gives thread
+  // t its 2^(3-j) twiddles as vectors of v = min(2^(3-j), 4) words at
+  // v (g NT + t), group g.
   static constexpr uint32_t CTILE_ENTRIES = 8190u;
   // staged twiddle bytes in shared memory, CTAs per SM
   static constexpr uint32_t SMEM_TW_BYTES =
@@ -252,6 +257,11 @@ struct TPass {
     } else if constexpr (LSTAGE && KD == Kind::S) {  // tw[L][pos mod 2^L] from the chunk's staged copy
       const uint32_t em = (1u << beta) - 1u;
       return tws[32u * em + ((((ct >> 5) & em) + ((cm >> 5) & em)) << 5) + (ct & 31u)];
+    } else if constexpr (LSTAGE && KD == Kind::C) {  // M31: the tile's staged table-order copy (w' = 2w + (w >> 30))
+      static_assert(!kStageThreadOrder, "12-layer rounds take their staged twiddles in round()");
+      const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (8192u - (8192u >> L));
+      const uint32_t ws = tw32[(ct >> (L + 1)) + (cm >> (L + 1))];
+      return make_uint2(ws >> 1, ws);
     } else if constexpr (F::kMontgomery) {  // BabyBear strided, per position: tw[L][pos mod 2^L]
       const uint2* base = a.tw + ((1u << L) - 1u);
       const uint32_t em = (1u << beta) - 1u;
@@ -291,7 +301,7 @@ struct TPass {
         if constexpr (LSTAGE) {
           // this thread's 2^(r-1-j) twiddles of layer j (a constant once unrolled)
           const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (8192u - (8192u >> L));
-          if constexpr (k == 0) {  // thread-ordered first-round layers
+          if constexpr (k == 0 && kStageThreadOrder) {  // thread-ordered first-round layers
             switch (r - 1 - j) {
               case 3: staged_w<4, 0>(tw32 + 4u * tid, tv); staged_w<4, 4>(tw32 + 4u * (NT + tid), tv); break;
               case 2: staged_w<4, 0>(tw32 + 4u * tid, tv); break;
@@ -662,6 +672,20 @@ struct TPass {
   static_assert(!HALVES || halves_ok(), "independent halves: contiguous tiles whose top bit is thread bit 8");
   static constexpr uint32_t HWORDS = TWORDS / 2, HBYTES = TBYTES / 2, HROWS = HWORDS / 32;
 
+  // M31 per-block twiddles (Shoup companions) of every layer L < P over tile
+  // positions [pos_base, pos_base + 2^13), all in table order: 2^(12-L)
+  // consecutive entries of layer L at 8192 - (8192 >> L).
+  __device__ static __forceinline__ void stage_ctile_plain(uint32_t* dst, const TmaArgs& a, uint32_t pos_base,
+                                                           uint32_t tid) {
+    const uint32_t n = 1u << a.log_n;
+    const uint32_t end = 8192u - (8192u >> P);
+    for (uint32_t e = tid; e < end; e += NT) {
+      const uint32_t L = 12u - (31u - __clz(8191u - e));  // e in [8192 - 2^(13-L), 8192 - 2^(12-L))
+      const uint32_t local = e - (8192u - (8192u >> L));
+      dst[e] = __ldg(&a.tw[(n - (n >> L)) + (pos_base >> (L + 1)) + local].y);
+    }
+  }
+
   __device__ static void run_halves(const CUtensorMap* min, const CUtensorMap* mout, const TmaArgs& args) {
     extern __shared__ __align__(1024) uint32_t smem_words[];
     const uint32_t tid = threadIdx.x;
@@ -792,8 +816,10 @@ struct TPass {
         // positions are a function of t, the same for the whole CTA).
         const uint32_t key = (KD == Kind::C) ? g.pos_base : ((uint32_t)g.s1 >> 1);
         if (key != staged) {
-          if constexpr (KD == Kind::C) {
+          if constexpr (kStageThreadOrder) {
             stage_ctile(reinterpret_cast<uint32_t*>(tws), a, g.pos_base, tid);
+          } else if constexpr (KD == Kind::C) {
+            stage_ctile_plain(reinterpret_cast<uint32_t*>(tws), a, g.pos_base, tid);
           } else {  // both chunks of the pair
             stage_lchunk(tws, a.tw, a.lo, 2u * key, tid);
             stage_lchunk(tws + LCHUNK_ENTRIES, a.tw, a.lo, 2u * key + 1u, tid);

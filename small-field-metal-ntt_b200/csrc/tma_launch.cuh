@@ -26,7 +26,7 @@ struct TmaRequest {
   bool twist_compact = false;    // the twist table holds Shoup companions only (TmaArgs::twist_compact)
   bool plain = false;            // BabyBear strided pass: plain sub-transform (twist by neighbours)
   // per-position twiddles staged in shared memory, one CTA per SM walking the
-  // columns (BabyBear 8-layer strided or M31 12-layer contiguous passes, n >= 2^13)
+  // columns (BabyBear 8-layer strided or M31 contiguous passes, n >= 2^13)
   bool lstage = false;
 };
 
@@ -139,7 +139,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
           if (ctx->c_halves) return launch_tma_pass<F, DESC, Kind::C, PP, false, true, false, true>(ctx, r, s); \
         return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);                    \
       }                                                                                          \
-    } else if constexpr (PP == 12) {                                                             \
+    } else {                                                                                     \
       if (r.lstage && r.log_n >= kTileBits)                                                      \
         return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);             \
     }                                                                                            \

@@ -366,3 +366,32 @@ def test_large_lde_multi_pass_layers(ctx, log_n, batch, added):
         rev = lambda bits: np.array([int(format(k, f"0{bits}b")[::-1], 2) for k in range(1 << bits)])
         nat = sfntt.CosetLdeBatch(ctx, natural=True).execute(x[rev(log_n)], log_n, 1, added).data
         assert np.array_equal(nat, r.data[rev(log_n + added)])
+
+
+@pytest.mark.parametrize("log_n", [13, 14, 15, 17, 18, 19])
+def test_m31_batch_staged_any_layer_count(ctx, log_n):
+    """M31 contiguous passes of 5..12 layers over >= 16 columns stage each
+    tile's per-block twiddles once for all its columns (table order for
+    layer counts other than 12): every column against the oracle, and the
+    round trip."""
+    batch = 16
+    b = sfntt.CudaCtGsR4(ctx)
+    x = data(M31, batch << log_n, 1900 + log_n)
+    fw, _ = b.forward_ntt_batch_gpu(x, log_n, batch)
+    n = 1 << log_n
+    for c in range(batch):
+        assert np.array_equal(fw[c * n:(c + 1) * n], O.m31_forward(x[c * n:(c + 1) * n])), c
+    back, _ = b.inverse_ntt_batch_gpu(fw, log_n, batch)
+    assert np.array_equal(back, x)
+
+
+def test_m31_lde_staged_multi_pass(ctx):
+    """M31 blow-up 2^21 x 17, 4x: the 13-layer ranges run as a staged 5-layer
+    contiguous pass and an 8-layer strided pass; sampled columns against the
+    oracle."""
+    log_n, batch, added = 21, 17, 2
+    n, n_ext = 1 << log_n, 1 << (log_n + added)
+    x = O.lcg(batch << log_n, 2121, O.M31_P)
+    r = sfntt.M31Lde(ctx).execute(x, log_n, batch, added)
+    for c in (0, 9, batch - 1):
+        assert np.array_equal(r.data[c * n_ext:(c + 1) * n_ext], O.m31_lde(x[c * n:(c + 1) * n], log_n, 1, added)), c
