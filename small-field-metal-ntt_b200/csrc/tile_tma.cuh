@@ -941,9 +941,11 @@ struct TExpand {
   __device__ static __forceinline__ bool tile_body(uint32_t* cur, uint32_t* ostage, const TmaArgs& ai,
                                                    const uint2* tws_inv, const uint2* tws_fwd, uint32_t t, bool ok,
                                                    const CUtensorMap* mout, uint32_t tid) {
+#ifndef SFNTT_NO_X_PAIRS  // (build-time switch for comparisons: one block at a time)
     if constexpr (F::kMontgomery && K == 2 && !PLAIN) {
       if (ai.log_q >= 1) return tile_body_pairs(cur, ostage, ai, tws_inv, tws_fwd, t, ok, mout, tid);
     }
+#endif
     using M = RM<Kind::S, P, LT, R, K - 1>;
     const uint32_t ct = M::ctid(tid);
     const uint32_t n = 1u << ai.log_n;
