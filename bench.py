@@ -988,16 +988,18 @@ def run_table(a) -> None:
         else:
             O.m31_lde(col, it["log_n"], 1, it["added_bits"], threads=1)
         cpu_1t += (time.perf_counter() - t) * it["batch"]
-    res["C4"] = {"gpu_plain_ms": un["plain_loop_ms"], "gpu_graph_ms": un["graph_ms"], "gpu_hbm_frac": un["hbm_frac"],
-                 "outputs_identical": un["outputs_identical"], "cpu_1t_ms": cpu_1t * 1e3}
+    res["C4"] = {"gpu_plain_ms": un["plain_loop_ms"], "gpu_graph_ms": un["graph_ms"],
+                 "gpu_persistent_ms": un["persistent_ms"], "gpu_hbm_frac": un["hbm_frac"],
+                 "outputs_identical": un["outputs_identical"] and un["persistent_outputs_identical"],
+                 "cpu_1t_ms": cpu_1t * 1e3}
     # C5
     sv = served_sweep(a, ctx, sfntt, torch)
-    res["C5"] = {"at_max_rate": sv["at_max_rate"],
-                 "sweep": [{"rate": r["rate_req_s"], "plain_p50_ms": r["plain"]["p50_ms"],
-                            "plain_p99_ms": r["plain"]["p99_ms"], "served_p50_ms": r["served"]["p50_ms"],
-                            "served_p99_ms": r["served"]["p99_ms"], "plain_melem_s": r["plain"]["melem_per_s"],
-                            "served_melem_s": r["served"]["melem_per_s"], "hbm_frac": r["served"]["hbm_frac"]}
-                           for r in sv["sweep"]]}
+    def rows(sweep):
+        return [{"rate": r["rate_req_s"], **{f"{m}_{k}": r[m][k] for m in ("plain", "served", "packed")
+                                              for k in ("p50_ms", "p99_ms", "melem_per_s")},
+                 "packed_hbm_frac": r["packed"]["hbm_frac"]} for r in sweep]
+    res["C5"] = {"at_max_rate": sv["at_max_rate"], "sweep": rows(sv["sweep"]),
+                 "small": {"at_max_rate": sv["small"]["at_max_rate"], "sweep": rows(sv["small"]["sweep"])}}
     print(json.dumps({"metric": "measurement table (C1-C5)", "rows": res, "device": ctx.device_info()}), flush=True)
 
 
