@@ -216,8 +216,8 @@ Status launch_tma_expand_c(sfntt_ctx* ctx, const uint32_t* src, uint32_t* d_out,
   using X = TExpandC<F>;
   const uint64_t n = 1ull << log_n;
   CUtensorMap min, mout;
-  SFNTT_TRY(encode_c_map(&min, src, log_n, n, batch));
-  SFNTT_TRY(encode_c_map(&mout, d_out, log_n + 1, 2 * n, batch));
+  SFNTT_TRY(encode_c_map(&min, src, log_n, n, batch, 12));
+  SFNTT_TRY(encode_c_map(&mout, d_out, log_n + 1, 2 * n, batch, 12));
   TmaArgs a{};
   a.tw = tw_inv;
   a.tw_fwd = tw_fwd;

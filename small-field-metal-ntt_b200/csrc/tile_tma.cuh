@@ -28,11 +28,23 @@ constexpr uint32_t kTileWords = 1u << kTileBits;
 constexpr uint32_t kTileBytes = 4u << kTileBits;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s: far beyond any tile's latency
 
-// Contiguous tiles are moved with the 128-byte TMA swizzle: word c of the tile
-// sits at c ^ (((c >> 5) & 7) << 2) in shared memory.  Without it, rounds whose
-// threads own tile bits 0..3 (four consecutive words, 128-bit accesses) hit
-// 4-way bank conflicts; with it every round but one is conflict-free.
+// Contiguous tiles are moved with the 128-byte TMA swizzle: word s of the
+// shared-memory tile sits at s ^ (((s >> 5) & 7) << 2).  Without it, rounds
+// whose threads own tile bits 0..3 (four consecutive words, 128-bit accesses)
+// hit 4-way bank conflicts.
 constexpr bool kSwizzleC = true;
+
+// Row order of contiguous tiles in shared memory.  Tile word c (c0..c4: the
+// word in its 128-byte row, c5..c12: the row) sits at shared word s = lay(c):
+// in row order (s = c) the bank of a word is (c0, c1, c2^c5, c3^c6, c4^c7), so
+// a round whose slots own tile bits 4..7 (the middle round of 8-, 11- and
+// 12-layer passes; lanes on bits 0..3 and 8) reaches only 16 banks: two-way
+// conflicts on every access.  Those passes store the rows as
+// [c5 c6][c8 .. c11][c7][c12] instead -- bank (c0, c1, c2^c5, c3^c6, c4^c8),
+// conflict-free in every round -- by loading each half tile (c12 fixed)
+// through a 5-dimensional tensor map (32 words, rows c5..c6, rows c8 and up,
+// row c7, column).  Other layer counts are conflict-free in row order.
+__host__ __device__ constexpr bool c_row_perm(int P) { return P == 8 || P == 11 || P == 12; }
 
 struct TmaArgs {
   const uint2* tw;     // twiddles (layer-concatenated Shoup pairs)
@@ -178,13 +190,36 @@ struct TPass {
   }
 
   __device__ static __forceinline__ void tma_load(const CUtensorMap* m, const Geo& g, uint32_t* dst, uint64_t* bar) {
-    if constexpr (KD == Kind::C) tma::load_3d(dst, m, 0, g.c1, g.c2, bar);
+    if constexpr (KD == Kind::C) c_load(m, g.c1, g.c2, dst, bar, true);
     else tma::load_5d(dst, m, 0, g.s1, 0, g.s3, g.s4, bar);
   }
 
   __device__ static __forceinline__ void tma_store(const CUtensorMap* m, const Geo& g, const uint32_t* src) {
-    if constexpr (KD == Kind::C) tma::store_3d(m, 0, g.c1, g.c2, src);
+    if constexpr (KD == Kind::C) c_store(m, g.c1, g.c2, src, true);
     else tma::store_5d(m, 0, g.s1, 0, g.s3, g.s4, src);
+  }
+
+  // Contiguous tiles: the whole tile at 128-byte row `row` of column `col`
+  // (rows [row, row + 256)), or the half tile there (rows [row, row + 128)).
+  // A row-ordered map's box is the copy (whole or half, as encoded); a
+  // row-permuted map's box is a half tile, so a whole tile takes two copies.
+  __device__ static __forceinline__ void c_load(const CUtensorMap* m, int32_t row, int32_t col, uint32_t* dst,
+                                                uint64_t* bar, bool whole) {
+    if constexpr (kRowPerm) {
+      tma::load_5d(dst, m, 0, 0, row >> 3, 0, col, bar);
+      if (whole) tma::load_5d(dst + TWORDS / 2, m, 0, 0, (row >> 3) + 16, 0, col, bar);
+    } else {
+      tma::load_3d(dst, m, 0, row, col, bar);
+    }
+  }
+  __device__ static __forceinline__ void c_store(const CUtensorMap* m, int32_t row, int32_t col, const uint32_t* src,
+                                                 bool whole) {
+    if constexpr (kRowPerm) {
+      tma::store_5d(m, 0, 0, row >> 3, 0, col, src);
+      if (whole) tma::store_5d(m, 0, 0, (row >> 3) + 16, 0, col, src + TWORDS / 2);
+    } else {
+      tma::store_3d(m, 0, row, col, src);
+    }
   }
 
   // BabyBear passes read their twiddles from a shared-memory copy of layers
@@ -433,11 +468,23 @@ struct TPass {
     return mp.mpos[0] == 0 && mp.mpos[1] == 1;
   }
 
-  // Shared-memory word of tile word c (the TMA layout of this tile kind).
+  // Shared-memory word of tile word c (the TMA layout of this tile kind: the
+  // row order of c_row_perm, then the swizzle).
   static constexpr bool kSwz = (KD == Kind::C) && kSwizzleC;
-  __host__ __device__ static constexpr uint32_t sw(uint32_t c) { return kSwz ? c ^ (((c >> 5) & 7u) << 2) : c; }
+  static constexpr bool kRowPerm = (KD == Kind::C) && c_row_perm(P);
+  __host__ __device__ static constexpr uint32_t lay(uint32_t c) {
+    return kRowPerm ? ((c & ~0xF80u) | ((c >> 1) & 0x780u) | ((c & 0x80u) << 4)) : c;
+  }
+  __host__ __device__ static constexpr uint32_t sw(uint32_t c) {
+    return kSwz ? (lay(c) ^ (((lay(c) >> 5) & 7u) << 2)) : c;
+  }
   // Bits that sw(x) may set when x ranges over the bits of `mask`.
-  __host__ __device__ static constexpr uint32_t sw_support(uint32_t mask) { return sw(mask) | mask; }
+  __host__ __device__ static constexpr uint32_t sw_support(uint32_t mask) {
+    uint32_t s = 0;
+    for (int i = 0; i < 32; ++i)
+      if ((mask >> i) & 1u) s |= sw(1u << i);
+    return s;
+  }
   // sw is linear over GF(2), so sw(ct | cm) = sw(ct) ^ sw(cm).  Round k's
   // thread part and slot part overlap only in the bits `overlap<k>()`; the
   // rest of sw(cm) is added as an immediate offset:
@@ -711,7 +758,7 @@ struct TPass {
     if (leader) {
       const Geo g0 = geo(a, t);
       tma::mbar_expect_tx(&bar[0], HBYTES);
-      tma::load_3d(stage, min, 0, g0.c1 + hrow, g0.c2, &bar[0]);
+      c_load(min, g0.c1 + hrow, g0.c2, stage, &bar[0], false);
     }
     const uint32_t bar_id = 3u + half;  // named barriers 1, 2 are the rounds' exchanges
     uint32_t v[E];
@@ -725,7 +772,7 @@ struct TPass {
         tma::wait_reads();  // the store that last used the other buffer has read it
         const Geo gn = geo(a, tn);
         tma::mbar_expect_tx(&bar[buf ^ 1u], HBYTES);
-        tma::load_3d(stage + (buf ^ 1u) * HWORDS, min, 0, gn.c1 + hrow, gn.c2, &bar[buf ^ 1u]);
+        c_load(min, gn.c1 + hrow, gn.c2, stage + (buf ^ 1u) * HWORDS, &bar[buf ^ 1u], false);
       }
       const Geo g = geo(a, t);
       const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
@@ -753,7 +800,7 @@ struct TPass {
         return;
       }
       if (leader) {
-        tma::store_3d(mout, 0, g.c1 + hrow, g.c2, cur);
+        c_store(mout, g.c1 + hrow, g.c2, cur, false);
         tma::commit();
       }
     }
@@ -1259,8 +1306,8 @@ struct TExpandC {
       }
       if (tid == 0) {
         // extended rows [2 * pos_base, 2 * pos_base + 2^14) of the column, two boxes of 2^13 words
-        tma::store_3d(mout, 0, 2 * g.c1, g.c2, ostage);
-        tma::store_3d(mout, 0, 2 * g.c1 + (int32_t)(TWORDS / 32), g.c2, ostage + TWORDS);
+        Inv::c_store(mout, 2 * g.c1, g.c2, ostage, true);
+        Inv::c_store(mout, 2 * g.c1 + (int32_t)(TWORDS / 32), g.c2, ostage + TWORDS, true);
         tma::commit();
       }
     }

@@ -52,20 +52,28 @@ inline bool tma_pass_ok(const TmaRequest& r) {
   return r.P >= 1 && r.P <= 8 && r.lo >= 5 && r.lo + r.P <= r.log_n;
 }
 
-// box_rows: 128-byte rows per copy (a whole 2^13-word tile, or half of one
-// for passes that run independent halves).
+// Contiguous tiles of a P-layer pass.  Row order (c_row_perm(P) false):
+// box_rows 128-byte rows per copy (a whole 2^13-word tile, or half of one for
+// passes that run independent halves).  Row-permuted: a half tile per copy,
+// its rows in the order [r0 r1][r3 ..][r2] of the row index r (dims: 32
+// words, rows r0..r1, rows r3 and up, row r2, column), whatever box_rows says.
 inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n, uint64_t stride, uint32_t batch,
-                           uint32_t box_rows = kTileWords / 32) {
+                           int P, uint32_t box_rows = kTileWords / 32) {
   const uint64_t n = 1ull << log_n;
-  cuuint64_t dims[3], strides[2];
-  const cuuint32_t box[3] = {32, box_rows, 1};
-  if (n >= kTileWords) {
-    dims[0] = 32; dims[1] = n / 32; dims[2] = batch;
-    strides[0] = 128; strides[1] = stride * 4;
-  } else {
-    dims[0] = 32; dims[1] = (uint64_t)batch * n / 32; dims[2] = 1;
-    strides[0] = 128; strides[1] = (uint64_t)batch * n * 4;
+  // rows per column and the column stride (dense columns shorter than a tile
+  // are one long column)
+  const uint64_t rows = n >= kTileWords ? n / 32 : (uint64_t)batch * n / 32;
+  const uint64_t cols = n >= kTileWords ? batch : 1;
+  const uint64_t col_bytes = n >= kTileWords ? stride * 4 : (uint64_t)batch * n * 4;
+  if (c_row_perm(P)) {
+    const cuuint64_t dims[5] = {32, 4, rows / 8, 2, cols};
+    const cuuint64_t strides[4] = {128, 1024, 512, col_bytes};
+    const cuuint32_t box[5] = {32, 4, kTileWords / 32 / 16, 2, 1};
+    return tensor_map_encode(m, base, 5, dims, strides, box, kSwizzleC);
   }
+  const cuuint64_t dims[3] = {32, rows, cols};
+  const cuuint64_t strides[2] = {128, col_bytes};
+  const cuuint32_t box[3] = {32, box_rows, 1};
   return tensor_map_encode(m, base, 3, dims, strides, box, kSwizzleC);
 }
 
@@ -105,8 +113,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   a.twist_compact = r.twist_compact ? 1u : 0u;
   if constexpr (KD == Kind::C) {
     const uint32_t rows = HALVES ? T::HROWS : kTileWords / 32;
-    SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch, rows));
-    SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch, rows));
+    SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch, P, rows));
+    SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch, P, rows));
     a.spans = n < kTileWords;
     a.log_tpc = a.spans ? 0u : r.log_n - kTileBits;
     // every M31 table with n >= 2^13 carries its first-round copy from entry n on

@@ -75,13 +75,33 @@ __device__ __forceinline__ void c_dispatch(int field, int P, uint32_t* cur, cons
 }
 #undef SFNTT_WL_C
 
+// TMA copies of an item's contiguous tiles.  The tile geometry is field- and
+// layer-independent; the copy form is not: 8-, 11- and 12-layer passes keep
+// their tiles row-permuted (a 5-dimensional map, half a tile per copy), the
+// others in row order (a 3-dimensional map) -- c_row_perm decides both here
+// and where worklist_add encodes the item's maps.
+template <bool DESC>
+struct CCopy {
+  using Perm = TPass<BabyBear, DESC, Kind::C, 12>;
+  using Rows = TPass<BabyBear, DESC, Kind::C, 10>;
+  static_assert(Perm::kRowPerm && !Rows::kRowPerm, "one copy form each");
+  __device__ static __forceinline__ void load(const WorkItem& w, uint32_t t, uint32_t* dst, uint64_t* bar) {
+    if (c_row_perm(w.P)) Perm::tma_load(&w.min, Perm::geo(w.a, t), dst, bar);
+    else Rows::tma_load(&w.min, Rows::geo(w.a, t), dst, bar);
+  }
+  __device__ static __forceinline__ void store(const WorkItem& w, uint32_t t, const uint32_t* src) {
+    if (c_row_perm(w.P)) Perm::tma_store(&w.mout, Perm::geo(w.a, t), src);
+    else Rows::tma_store(&w.mout, Rows::geo(w.a, t), src);
+  }
+};
+
 // Contiguous passes of every item (layers [0, P_item) of its network):
 // 2^13-word tiles, the same geometry for every layer count.
 template <bool DESC>
 __global__ void __launch_bounds__(512, 2)
 worklist_c_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict__ units, uint32_t n_units,
                   uint32_t* counter, const uint2* bb_tw) {
-  using G = TPass<BabyBear, DESC, Kind::C, 12>;  // tile geometry and TMA (field- and layer-independent)
+  using G = CCopy<DESC>;
   extern __shared__ __align__(1024) uint32_t smem_words[];
   uint32_t* stage = smem_words;
   uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 2 * kTileWords);
@@ -102,7 +122,7 @@ worklist_c_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
     if (next_tile(cursor, units, n_units, counter, item, t)) {
       const WorkItem& w = items[item];
       tma::mbar_expect_tx(&bar[0], kTileBytes);
-      G::tma_load(&w.min, G::geo(w.a, t), stage, &bar[0]);
+      G::load(w, t, stage, &bar[0]);
       slot[0] = item;
       slot[2] = t;
     } else {
@@ -124,7 +144,7 @@ worklist_c_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
         tma::wait_reads();  // the store that last used the other buffer has read it
         const WorkItem& wn = items[ni];
         tma::mbar_expect_tx(&bar[buf ^ 1u], kTileBytes);
-        G::tma_load(&wn.min, G::geo(wn.a, nt), stage + (buf ^ 1u) * kTileWords, &bar[buf ^ 1u]);
+        G::load(wn, nt, stage + (buf ^ 1u) * kTileWords, &bar[buf ^ 1u]);
         slot[buf ^ 1u] = ni;
         slot[2 + (buf ^ 1u)] = nt;
         issued = true;
@@ -145,7 +165,7 @@ worklist_c_kernel(const WorkItem* __restrict__ items, const WorkUnit* __restrict
       return;
     }
     if (tid == 0) {
-      G::tma_store(&w.mout, G::geo(w.a, t), cur);
+      G::store(w, t, cur);
       tma::commit();
     }
   }
@@ -345,8 +365,8 @@ Status worklist_add(sfntt_ctx* ctx, WorkPhase& ph, int phase, const sfntt_lde_it
     const uint64_t nn = 1ull << lg;
     const uint32_t* in = desc ? it.d_out : it.d_in;
     const uint64_t in_stride = desc ? n_ext : n;
-    SFNTT_TRY(encode_c_map(&w.min, in, lg, in_stride, it.batch));
-    SFNTT_TRY(encode_c_map(&w.mout, it.d_out, lg, n_ext, it.batch));
+    SFNTT_TRY(encode_c_map(&w.min, in, lg, in_stride, it.batch, (int)lo));
+    SFNTT_TRY(encode_c_map(&w.mout, it.d_out, lg, n_ext, it.batch, (int)lo));
     a.tw = desc ? tw_fwd : tw_inv;
     a.log_n = lg;
     a.lo = 0;
