@@ -130,6 +130,10 @@ struct sfntt_ctx {
   // contiguous 8- and 12-layer TMA passes run their two CTA halves as
   // independent pipelines (half tiles, own barriers); off: whole tiles
   bool c_halves = true;
+  // persistent batches: items of at most this many tiles (2^13 input words)
+  // join the work-list phases; larger items fill the GPU on their own and run
+  // per item beside them.  -1: 16 tiles per SM; 0: no limit.
+  int64_t worklist_max_tiles = -1;
   // autotuned plans: "field/log_n/columns/added_bits" -> sfntt_plan
   std::map<std::string, int> tuned;
 

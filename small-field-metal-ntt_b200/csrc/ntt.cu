@@ -14,13 +14,14 @@ namespace sfntt {
 
 // TMA plan for layers [0, b): one contiguous pass, then strided passes of at
 // most 8 layers.  Default: the strided passes take 8 layers each and the
-// contiguous pass the rest (5..12 layers).  c12_first (a tuning knob, for
-// b > 12): the contiguous pass takes 12 layers and the strided passes share
-// the rest as evenly as possible (b = 14: 12 + 2 instead of 6 + 8).
+// contiguous pass the rest (5..13 layers: b = 13 and b = 21 need one pass
+// fewer than with at most 12).  c12_first (a tuning knob, for b > 12): the
+// contiguous pass takes 12 layers and the strided passes share the rest as
+// evenly as possible (b = 14: 12 + 2 instead of 6 + 8).
 int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first) {
   if (a != 0) return 0;
-  const uint32_t s = b > 12 ? (b - 12 + 7) / 8 : 0;
-  if (c12_first && s > 0) {
+  if (c12_first && b > 12) {
+    const uint32_t s = (b - 12 + 7) / 8;
     if (s > 3) return 0;
     const uint32_t rest = b - 12;
     lo[0] = 0;
@@ -33,8 +34,9 @@ int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_
     }
     return (int)(1 + s);
   }
+  const uint32_t s = b > 13 ? (b - 13 + 7) / 8 : 0;
   const uint32_t c = b - 8 * s;
-  if (c < 5 || c > 12 || s > 3) return 0;
+  if (c < 5 || c > 13 || s > 3) return 0;
   lo[0] = 0;
   cnt[0] = c;
   for (uint32_t i = 1; i <= s; ++i) { lo[i] = c + 8 * (i - 1); cnt[i] = 8; }

@@ -243,7 +243,11 @@ struct TPass {
   // in table order.
   static constexpr bool kStageThreadOrder = LSTAGE && KD == Kind::C && P == 12;
   static_assert(!kStageThreadOrder || kRound0Copy, "M31 tile staging starts from the first-round copy");
-  static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << P) - 1u) : 0u;
+  // BabyBear staged twiddles: layers [0, min(P, 12)) (32 KiB at most, two CTAs
+  // per SM); a 13-layer contiguous pass reads its top layer's 4096 twiddles
+  // from the global table.
+  static constexpr int kStagedLayers = P < 12 ? P : 12;
+  static constexpr uint32_t TW_ENTRIES = kStaged ? ((1u << kStagedLayers) - 1u) : 0u;
   // M31 tile staging: the twiddles of a tile's 2^13 positions, one word each
   // -- the Shoup companion w' = floor(w 2^32 / p), which for the Mersenne
   // prime (2^32 / p = 2 + 2 / p) is 2w + (w >= 2^30), so w = w' >> 1, one
@@ -285,10 +289,13 @@ struct TPass {
     const uint32_t cm = M::cm(m);
     const uint32_t L = a.lo + beta;
     if constexpr (kStaged) {
-      const uint2* base = tws + ((1u << beta) - 1u);
       const uint32_t mask = (1u << beta) - 1u;
-      if constexpr (KD == Kind::C) return base[(ct & mask) + (cm & mask)];
-      else return base[((ct >> 5) & mask) + ((cm >> 5) & mask)];
+      if constexpr (KD == Kind::C) {
+        if (beta >= (uint32_t)kStagedLayers) return __ldg(a.tw + ((1u << beta) - 1u) + (ct & mask) + (cm & mask));
+        return tws[((1u << beta) - 1u) + (ct & mask) + (cm & mask)];
+      } else {
+        return tws[((1u << beta) - 1u) + ((ct >> 5) & mask) + ((cm >> 5) & mask)];
+      }
     } else if constexpr (LSTAGE && KD == Kind::S) {  // tw[L][pos mod 2^L] from the chunk's staged copy
       const uint32_t em = (1u << beta) - 1u;
       return tws[32u * em + ((((ct >> 5) & em) + ((cm >> 5) & em)) << 5) + (ct & 31u)];
@@ -476,7 +483,8 @@ struct TPass {
     return kRowPerm ? ((c & ~0xF80u) | ((c >> 1) & 0x780u) | ((c & 0x80u) << 4)) : c;
   }
   __host__ __device__ static constexpr uint32_t sw(uint32_t c) {
-    return kSwz ? (lay(c) ^ (((lay(c) >> 5) & 7u) << 2)) : c;
+    const uint32_t s = lay(c);
+    return kSwz ? (s ^ (((s >> 5) & 7u) << 2)) : s;
   }
   // Bits that sw(x) may set when x ranges over the bits of `mask`.
   __host__ __device__ static constexpr uint32_t sw_support(uint32_t mask) {
@@ -551,8 +559,7 @@ struct TPass {
     }
     return -1;
   }
-  template <int kp, int k>
-  __host__ __device__ static constexpr int xfixed() {
+  __host__ __device__ static constexpr int xfixed_of(int kp, int k) {
     int mask = 0;
     for (int c = 0; c < CB; ++c) {
       const int a = tid_bit(kp, c), b = tid_bit(k, c);
@@ -563,15 +570,38 @@ struct TPass {
     }
     return mask;
   }
-  static constexpr int kWarpBits = (NT - 1) & ~31;
   template <int kp, int k>
+  __host__ __device__ static constexpr int xfixed() { return xfixed_of(kp, k); }
+  static constexpr int kWarpBits = (NT - 1) & ~31;
+  __host__ __device__ static constexpr int popc(int x) { return x ? (x & 1) + popc(x >> 1) : 0; }
+  // Named-barrier groups of the exchange between rounds kp and k (0: a warp
+  // or CTA barrier).
+  __host__ __device__ static constexpr int xgroups(int kp, int k) {
+    const int fixed = xfixed_of(kp, k);
+    const int wf = fixed < 0 ? 0 : (fixed & kWarpBits);
+    if (fixed >= 0 && kWarpBits != 0 && wf == kWarpBits) return 0;
+    return (wf != 0 && popc(wf) <= 3) ? (1 << popc(wf)) : 0;
+  }
+  // First barrier id of the exchange before rounds<i>.  Consecutive exchanges
+  // of one tile may group the warps differently with no CTA barrier between
+  // them, so a warp can reach the next exchange's barrier while others still
+  // wait at this one: every exchange of the pass takes its own ids (1 + the
+  // groups of the exchanges before it; ids 14 and 15 are the independent
+  // halves' pre-store barriers).
+  __host__ __device__ static constexpr int xbase(int i) {
+    int b = 1;
+    for (int j = 1; j < i; ++j) b += DESC ? xgroups(K - j, K - 1 - j) : xgroups(j - 1, j);
+    return b;
+  }
+  template <int kp, int k, int BASE>
   __device__ static __forceinline__ void xsync(uint32_t tid) {
     constexpr int fixed = xfixed<kp, k>();
     constexpr int wf = fixed < 0 ? 0 : (fixed & kWarpBits);
     if constexpr (fixed >= 0 && kWarpBits != 0 && wf == kWarpBits) {
       __syncwarp();
     } else if constexpr (wf != 0 && __builtin_popcount(wf) <= 3) {
-      uint32_t id = 1, i = 0;
+      static_assert(BASE + (1 << __builtin_popcount(wf)) - 1 <= 13, "named barrier ids of the exchanges: 1..13");
+      uint32_t id = BASE, i = 0;
 #pragma unroll
       for (int bit = 5; bit < 16; ++bit) {
         if ((wf >> bit) & 1) {
@@ -596,7 +626,7 @@ struct TPass {
       if constexpr (i > 0) {
         constexpr int kp = DESC ? (K - i) : (i - 1);
         st<kp>(buf, v, tid);
-        xsync<kp, k>(tid);
+        xsync<kp, k, xbase(i)>(tid);
         ld<k>(buf, v, tid);
       }
       round<k>(v, a, tws, g, tid);
@@ -760,7 +790,7 @@ struct TPass {
       tma::mbar_expect_tx(&bar[0], HBYTES);
       c_load(min, g0.c1 + hrow, g0.c2, stage, &bar[0], false);
     }
-    const uint32_t bar_id = 3u + half;  // named barriers 1, 2 are the rounds' exchanges
+    const uint32_t bar_id = 14u + half;  // named barriers 1..13 are the rounds' exchanges
     uint32_t v[E];
     for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
       const uint32_t buf = it & 1u;
@@ -912,6 +942,10 @@ static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<2, 1>() == 0x10F, "C12 
 static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<1, 0>() == 0x1F0, "C12 1->0: tid bits 4-8 (in a warp)");
 static_assert(TPass<BabyBear, false, Kind::C, 8>::xfixed<0, 1>() == 0x1F0, "C8 0->1: in a warp");
 static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: lanes only, whole CTA");
+// 13-layer passes: two grouped exchanges in a row (4 groups each), on disjoint ids
+static_assert(TPass<BabyBear, false, Kind::C, 13>::xgroups(1, 2) == 4 && TPass<BabyBear, false, Kind::C, 13>::xgroups(2, 3) == 4 &&
+                  TPass<BabyBear, false, Kind::C, 13>::xbase(3) == 5 && TPass<BabyBear, true, Kind::C, 13>::xbase(2) == 5,
+              "C13 exchange barrier ids");
 
 // BabyBear LSTAGE passes stage 64 KiB of twiddles besides the two tiles (one
 // CTA per SM); M31 contiguous ones 32 KiB (two).

@@ -45,7 +45,7 @@ inline bool tma_pass_ok(const TmaRequest& r) {
   if (!aligned16(r.in) || !aligned16(r.out) || (r.in_stride & 3) || (r.out_stride & 3)) return false;
   const uint64_t n = 1ull << r.log_n;
   if (r.contiguous) {
-    if (r.P < 5 || r.P > 12 || r.lo != 0) return false;
+    if (r.P < 5 || r.P > 13 || r.lo != 0) return false;
     if (n >= kTileWords) return true;
     return r.in_stride == n && r.out_stride == n && ((uint64_t)r.batch * n) % kTileWords == 0;
   }
@@ -173,7 +173,7 @@ Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   if (r.contiguous) {
     switch (r.P) {
       SFNTT_TMA_C(5) SFNTT_TMA_C(6) SFNTT_TMA_C(7) SFNTT_TMA_C(8)
-      SFNTT_TMA_C(9) SFNTT_TMA_C(10) SFNTT_TMA_C(11) SFNTT_TMA_C(12)
+      SFNTT_TMA_C(9) SFNTT_TMA_C(10) SFNTT_TMA_C(11) SFNTT_TMA_C(12) SFNTT_TMA_C(13)
       default: break;
     }
   } else {

@@ -1,7 +1,7 @@
 // worklist.cu -- the persistent phase kernels of an uneven batch and the
 // host code that lays out their work list.
 //
-// Items of either field (BabyBear, M31) with 2^13 .. 2^20 points per column
+// Items of either field (BabyBear, M31) with 2^13 .. 2^21 points per column
 // and a blow-up of at most 16 run their LDE in three phases, each ONE launch
 // over every such item of the batch:
 //   phase 1: inverse layers [0, log n - 8) of every item (contiguous tiles),
@@ -63,12 +63,13 @@ __device__ __forceinline__ void c_dispatch(int field, int P, uint32_t* cur, cons
     switch (P) {
       SFNTT_WL_C(BabyBear, 5) SFNTT_WL_C(BabyBear, 6) SFNTT_WL_C(BabyBear, 7) SFNTT_WL_C(BabyBear, 8)
       SFNTT_WL_C(BabyBear, 9) SFNTT_WL_C(BabyBear, 10) SFNTT_WL_C(BabyBear, 11) SFNTT_WL_C(BabyBear, 12)
+      SFNTT_WL_C(BabyBear, 13)
       default: break;
     }
   } else {
     switch (P) {
       SFNTT_WL_C(M31, 5) SFNTT_WL_C(M31, 6) SFNTT_WL_C(M31, 7) SFNTT_WL_C(M31, 8)
-      SFNTT_WL_C(M31, 9) SFNTT_WL_C(M31, 10) SFNTT_WL_C(M31, 11) SFNTT_WL_C(M31, 12)
+      SFNTT_WL_C(M31, 9) SFNTT_WL_C(M31, 10) SFNTT_WL_C(M31, 11) SFNTT_WL_C(M31, 12) SFNTT_WL_C(M31, 13)
       default: break;
     }
   }
@@ -283,6 +284,7 @@ bool m31_round0_copy(bool desc, int P) {
       case 10: return TPass<M31, D, Kind::C, 10>::kRound0Copy;
       case 11: return TPass<M31, D, Kind::C, 11>::kRound0Copy;
       case 12: return TPass<M31, D, Kind::C, 12>::kRound0Copy;
+      case 13: return TPass<M31, D, Kind::C, 13>::kRound0Copy;
       default: return false;
     }
   };
@@ -300,9 +302,12 @@ bool worklist_eligible(const sfntt_ctx* ctx, const sfntt_lde_item& it) {
   if (ctx->no_tma || it.batch == 0) return false;
   if (it.field != SFNTT_BABYBEAR && it.field != SFNTT_M31) return false;
   if (it.plan != SFNTT_PLAN_AUTO && it.plan != SFNTT_PLAN_TMA) return false;
-  if (it.log_n < 13 || it.log_n > 20 || it.added_bits > 4) return false;
+  if (it.log_n < 13 || it.log_n > 21 || it.added_bits > 4) return false;
   if (it.field == SFNTT_BABYBEAR && ctx->lde_plain) return false;
-  if (((uint64_t)it.batch << it.log_n) >> kTileBits >= (1ull << 31)) return false;
+  const uint64_t tiles = ((uint64_t)it.batch << it.log_n) >> kTileBits;
+  if (tiles >= (1ull << 31)) return false;
+  const int64_t cap = ctx->worklist_max_tiles < 0 ? 16 * (int64_t)ctx->sm_count : ctx->worklist_max_tiles;
+  if (cap > 0 && tiles > (uint64_t)cap) return false;
   return aligned16(it.d_in) && aligned16(it.d_out);
 }
 

@@ -29,7 +29,7 @@ struct alignas(128) WorkItem {
   CUtensorMap mout;  // output map
   TmaArgs a;         // the pass's arguments (as the single-item launch sets them)
   int32_t field;     // SFNTT_BABYBEAR or SFNTT_M31
-  int32_t P;         // contiguous passes: layers 5..12; expansions: 8
+  int32_t P;         // contiguous passes: layers 5..13; expansions: 8
   uint32_t lstage;   // expansions: BabyBear twiddle chunks staged in shared memory
   uint32_t pad;
 };
@@ -49,8 +49,9 @@ struct WorkPhase {
   const uint2* bb_tw = nullptr;
 };
 
-// Items that the persistent phases run: BabyBear or M31, 2^13..2^20 points,
-// blow-up <= 16, TMA-aligned buffers, the default TMA plan.
+// Items that the persistent phases run: BabyBear or M31, 2^13..2^21 points,
+// blow-up <= 16, TMA-aligned buffers, the default TMA plan, and no more tiles
+// than the context's worklist_max_tiles (larger items fill the GPU alone).
 bool worklist_eligible(const sfntt_ctx* ctx, const sfntt_lde_item& it);
 // Appends the item's pass of `phase` (0: inverse layers [0, log n - 8),
 // 1: expansion, 2: forward layers [0, log n - 8) of the extended network).

@@ -598,7 +598,7 @@ class LdeBatch:
         return Graph(h)
 
     def persistent_graph(self, lanes: int = 8) -> "Graph":
-        """The batch with its eligible items (BabyBear / M31, 2^13..2^20
+        """The batch with its eligible items (BabyBear / M31, 2^13..2^21
         points, blow-up <= 16) in three persistent phase launches over a
         device work list, the rest per item on `lanes` streams, in one graph
         (sfntt_batch_persistent_create)."""

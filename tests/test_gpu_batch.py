@@ -141,14 +141,29 @@ def test_persistent_phases_match_oracle(ctx):
     g.close()
 
 
-def test_persistent_phases_large_items(ctx):
-    """2^20-point items of both fields with many columns (the staged BabyBear
-    expansion and 12-layer contiguous passes): sampled columns against the
-    oracle and the whole output against the per-item launches."""
+def test_persistent_phases_large_items():
+    """2^20- and 2^21-point items of both fields with many columns (the staged
+    BabyBear expansion, 12- and 13-layer contiguous passes): sampled columns
+    against the oracle and the whole output against the per-item launches."""
+    import os
     import torch
+    # a context whose work list takes items of any size (the default leaves
+    # items of more than 16 tiles per SM to their own launches)
+    old = os.environ.get("SFNTT_WORKLIST_TILES")
+    os.environ["SFNTT_WORKLIST_TILES"] = "0"
+    try:
+        ctx = sfntt.Context(0)
+    finally:
+        if old is None:
+            del os.environ["SFNTT_WORKLIST_TILES"]
+        else:
+            os.environ["SFNTT_WORKLIST_TILES"] = old
     items = [{"field": sfntt.FIELD_BABYBEAR, "log_n": 20, "batch": 24, "added_bits": 1},
              {"field": sfntt.FIELD_M31, "log_n": 19, "batch": 20, "added_bits": 2},
-             {"field": sfntt.FIELD_BABYBEAR, "log_n": 18, "batch": 5, "added_bits": 2}]
+             {"field": sfntt.FIELD_BABYBEAR, "log_n": 18, "batch": 5, "added_bits": 2},
+             # 2^21: 13-layer contiguous phases
+             {"field": sfntt.FIELD_M31, "log_n": 21, "batch": 18, "added_bits": 1},
+             {"field": sfntt.FIELD_BABYBEAR, "log_n": 21, "batch": 17, "added_bits": 1}]
     bufs = _alloc(items, 5100)
     batch = sfntt.LdeBatch(ctx, items)
     batch.prepare()

@@ -132,3 +132,45 @@ def test_bench_configuration_full_size(ctx):
         for i in (0, 1, 2, 3, 1000, n - 1):
             sh_i = O.bb_to_monty(pow(31, int(i), O.BB_P))
             assert int(lo[i]) == O.bb_mul(int(base[i]), sh_i), (c, i)
+
+
+# ---- 13-layer contiguous passes: 2^13 and 2^21 columns (one contiguous pass
+# of 13 layers, plus one 8-layer strided pass at 2^21), LDEs whose inverse and
+# forward low layers are 13 (log n = 21) ----------------------------------
+def _m31_batch(fn, x, log_n, batch):
+    n = 1 << log_n
+    return np.concatenate([fn(x[c * n:(c + 1) * n]) for c in range(batch)])
+
+
+@pytest.mark.parametrize("log_n,batch", [(13, 3), (21, 2)])
+def test_thirteen_layer_batches(ctx, log_n, batch):
+    import torch
+    n = 1 << log_n
+    xb = O.lcg(batch * n, 1300 + log_n, O.BB_P, monty=True)
+    xm = O.lcg(batch * n, 1400 + log_n, O.M31_P)
+    stream = torch.cuda.current_stream().cuda_stream
+    for eng, x, fwd, inv in ((sfntt.BbCudaCtGsR4(ctx), xb, lambda v: O.bb_forward_batch(v, log_n, batch, threads=8),
+                              lambda v: O.bb_inverse_batch(v, log_n, batch, threads=8)),
+                             (sfntt.CudaCtGsR4(ctx), xm, lambda v: _m31_batch(O.m31_forward, v, log_n, batch),
+                              lambda v: _m31_batch(O.m31_inverse, v, log_n, batch))):
+        d = torch.from_numpy(x.view(np.int32).copy()).cuda()
+        eng.forward_dev(d.data_ptr(), log_n, batch, stream=stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(d.cpu().numpy().view(np.uint32), fwd(x)), log_n
+        d.copy_(torch.from_numpy(x.view(np.int32).copy()))
+        eng.inverse_dev(d.data_ptr(), log_n, batch, stream=stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(d.cpu().numpy().view(np.uint32), inv(x)), log_n
+
+
+@pytest.mark.parametrize("batch", [2, 16])
+def test_lde_log_n_21(ctx, batch):
+    """BabyBear coset LDE and M31 blow-up at 2^21 (low layers: one 13-layer
+    contiguous pass each way); 16 columns take the M31 staged-twiddle passes."""
+    log_n, added = 21, 1
+    xb = O.lcg(batch << log_n, 2100 + batch, O.BB_P, monty=True)
+    r = sfntt.CosetLdeBatch(ctx).execute(xb, log_n, batch, added)
+    assert np.array_equal(r.data, O.bb_coset_lde(xb, log_n, batch, added, threads=8))
+    xm = O.lcg(batch << log_n, 2200 + batch, O.M31_P)
+    r = sfntt.M31Lde(ctx).execute(xm, log_n, batch, added)
+    assert np.array_equal(r.data, O.m31_lde(xm, log_n, batch, added, threads=8))
