@@ -263,7 +263,9 @@ int sfntt_batch_run(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, v
 int sfntt_batch_graph_create(sfntt_ctx *ctx, const sfntt_lde_item *items, size_t count, int lanes,
                              sfntt_graph **out);
 /* The same batch in persistent form: every BabyBear / M31 item with
- * 2^13..2^21 points, blow-up <= 16 and the default plan runs its LDE in three
+ * 2^13..2^21 points, blow-up <= 16, the default plan and at most 16 tiles
+ * (2^13 input words each) per SM (SFNTT_WORKLIST_TILES at context creation:
+ * another limit, 0 = none) runs its LDE in three
  * phases -- inverse low layers, expansion, forward low layers -- and each
  * phase is ONE persistent launch over all those items: its CTAs pop (item,
  * tile range) units from a work list in device memory (owned by the graph)
