@@ -616,6 +616,40 @@ struct TPass {
     }
   }
 
+  // Warp-shuffle form of an exchange (build-time switch SFNTT_SHFL_EXCHANGE,
+  // for comparisons).  Where round k's slot bit j is round kp's lane bit j and
+  // the reverse, for every j < R, and the other thread-id bits keep their tile
+  // bits, the exchange is a transpose of R slot bits with R lane bits inside a
+  // warp: R xor-shuffle stages, stage j swapping slot bit j with lane bit j (per
+  // slot pair one shuffle and three selects).  The contiguous 8-, 11- and
+  // 12-layer passes' warp-local exchanges have this form (checked on the CPU
+  // against the shared-memory exchange's word map).
+  __host__ __device__ static constexpr bool shfl_swap(int kp, int k) {
+    const RoundMap a = make_map<KD, P, LT, R>(kp), b = make_map<KD, P, LT, R>(k);
+    for (int j = 0; j < R; ++j)
+      if (tid_bit(k, a.mpos[j]) != j || tid_bit(kp, b.mpos[j]) != j) return false;
+    for (int c = 0; c < CB; ++c) {
+      const int ta = tid_bit(kp, c), tb = tid_bit(k, c);
+      if ((ta >= R || tb >= R) && ta != tb) return false;
+    }
+    return true;
+  }
+  __device__ static __forceinline__ void shfl_transpose(uint32_t (&v)[E], uint32_t tid) {
+    const uint32_t lane = tid & 31u;
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const bool hi = (lane >> j) & 1u;
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        if ((m >> j) & 1) continue;
+        const uint32_t send = hi ? v[m] : v[m | (1 << j)];
+        const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 1 << j);
+        if (hi) v[m] = recv;
+        else v[m | (1 << j)] = recv;
+      }
+    }
+  }
+
   // All K rounds starting from registers in round (DESC ? K-1 : 0)'s layout,
   // exchanging through `buf`; ends in round (DESC ? 0 : K-1)'s layout.
   template <int i>
@@ -625,9 +659,16 @@ struct TPass {
       constexpr int k = DESC ? (K - 1 - i) : i;
       if constexpr (i > 0) {
         constexpr int kp = DESC ? (K - i) : (i - 1);
-        st<kp>(buf, v, tid);
-        xsync<kp, k, xbase(i)>(tid);
-        ld<k>(buf, v, tid);
+#ifdef SFNTT_SHFL_EXCHANGE
+        if constexpr (shfl_swap(kp, k)) {
+          shfl_transpose(v, tid);
+        } else
+#endif
+        {
+          st<kp>(buf, v, tid);
+          xsync<kp, k, xbase(i)>(tid);
+          ld<k>(buf, v, tid);
+        }
       }
       round<k>(v, a, tws, g, tid);
       rounds<i + 1>(buf, v, a, tws, g, tid);
@@ -942,6 +983,10 @@ static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<2, 1>() == 0x10F, "C12 
 static_assert(TPass<BabyBear, true, Kind::C, 12>::xfixed<1, 0>() == 0x1F0, "C12 1->0: tid bits 4-8 (in a warp)");
 static_assert(TPass<BabyBear, false, Kind::C, 8>::xfixed<0, 1>() == 0x1F0, "C8 0->1: in a warp");
 static_assert(TPass<BabyBear, false, Kind::S, 8>::xfixed<0, 1>() == 0x1F, "S8: lanes only, whole CTA");
+static_assert(TPass<BabyBear, false, Kind::C, 12>::shfl_swap(0, 1) && TPass<BabyBear, true, Kind::C, 12>::shfl_swap(1, 0) &&
+                  TPass<BabyBear, false, Kind::C, 8>::shfl_swap(0, 1) && !TPass<BabyBear, false, Kind::C, 12>::shfl_swap(1, 2) &&
+                  !TPass<BabyBear, false, Kind::S, 8>::shfl_swap(0, 1),
+              "warp-local exchanges of the shuffle form");
 // 13-layer passes: two grouped exchanges in a row (4 groups each), on disjoint ids
 static_assert(TPass<BabyBear, false, Kind::C, 13>::xgroups(1, 2) == 4 && TPass<BabyBear, false, Kind::C, 13>::xgroups(2, 3) == 4 &&
                   TPass<BabyBear, false, Kind::C, 13>::xbase(3) == 5 && TPass<BabyBear, true, Kind::C, 13>::xbase(2) == 5,
