@@ -263,6 +263,7 @@ int sfntt_ctx_create(int device, sfntt_ctx** out) {
   if (const char* e = std::getenv("SFNTT_HALVES")) ctx->c_halves = e[0] != '0';
   if (const char* e = std::getenv("SFNTT_LDE_PLAIN")) ctx->lde_plain = e[0] == '1';
   if (const char* e = std::getenv("SFNTT_WORKLIST_TILES")) ctx->worklist_max_tiles = std::strtoll(e, nullptr, 10);
+  if (const char* e = std::getenv("SFNTT_SPLIT_C12")) ctx->split_c12 = e[0] == '1';
   bool ok = ctx->err.reserve(sizeof(int)).ok() && cudaMemset(ctx->err.p, 0, sizeof(int)) == cudaSuccess &&
             cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&ctx->copy_streams[0], cudaStreamNonBlocking) == cudaSuccess &&
