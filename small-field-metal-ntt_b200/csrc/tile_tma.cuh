@@ -261,6 +261,23 @@ struct TPass {
   static constexpr uint32_t SMEM_TW_BYTES =
       LSTAGE ? (KD == Kind::S ? 2u * 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
   static constexpr int kCtasPerSm = (LSTAGE && KD == Kind::S) ? 1 : 2;
+  // Tile buffers of the whole-tile pipeline (run): three -- the tiles two and
+  // one ahead in flight while one is computed -- for the staged strided passes
+  // (one CTA per SM, 227 KiB with the twiddle chunks: 2^20 x 256 natural-order
+  // LDE 3.72 -> 3.69 ms), else two.  Three buffers everywhere they fit at the
+  // same CTAs per SM (228 KiB per SM, 1 KiB reserved per CTA) was measured:
+  // the 2^24-point NTT's twisted strided pass went 45.8 -> 51.1 us (its twist
+  // and column compete for L2 with the extra tile in flight), the plain one
+  // 34.4 -> 32.0 us, the pair 213 -> 220 us.  The independent halves keep two
+  // half-tile buffers per half.
+  __host__ __device__ static constexpr int smem_bytes(int stages) {
+    return stages * (int)TBYTES + 32 + (int)SMEM_TW_BYTES + 1024;
+  }
+  static constexpr int kStages = (LSTAGE && KD == Kind::S && (smem_bytes(3) + 1024) * kCtasPerSm <= 233472 &&
+                                  smem_bytes(3) <= 232448)
+                                     ? 3
+                                     : 2;
+  static constexpr int kSmemBytes = smem_bytes(HALVES ? 2 : kStages);
 
   // C = 1, 2 or 4 consecutive staged M31 twiddles (Shoup companions) from
   // shared memory (p aligned to C words) into tv[AT, AT + C) as (w, w') pairs
@@ -886,9 +903,10 @@ struct TPass {
     // Dynamic shared memory is 1024-byte aligned; indexing it directly keeps
     // every access in the shared state space (LDS/STS, not generic LD/ST).
     extern __shared__ __align__(1024) uint32_t smem_words[];
+    constexpr uint32_t NS = (uint32_t)kStages;  // tile buffers: tile it in buffer it % NS
     uint32_t* stage = smem_words;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(stage + 2 * TWORDS);
-    uint2* tws = reinterpret_cast<uint2*>(bar + 2);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(stage + NS * TWORDS);
+    uint2* tws = reinterpret_cast<uint2*>(bar + 4);
     const uint32_t tid = threadIdx.x;
     const TmaArgs& a = args;
     uint32_t t, t_end, t_step;
@@ -907,25 +925,30 @@ struct TPass {
     if (tid == 0) {
       tma::prefetch_map(min);
       tma::prefetch_map(mout);
-      tma::mbar_init(&bar[0], 1);
-      tma::mbar_init(&bar[1], 1);
+      for (uint32_t b = 0; b < NS; ++b) tma::mbar_init(&bar[b], 1);
       tma::fence_mbar_init();
     }
     __syncthreads();
     if (tid == 0) {
-      tma::mbar_expect_tx(&bar[0], TBYTES);
-      tma_load(min, geo_run(a, t), stage, &bar[0]);
+      for (uint32_t b = 0; b + 1 < NS; ++b) {  // tiles 0 .. NS-2 of this CTA
+        const uint32_t tb = t + b * t_step;
+        if (tb < t_end) {
+          tma::mbar_expect_tx(&bar[b], TBYTES);
+          tma_load(min, geo_run(a, tb), stage + b * TWORDS, &bar[b]);
+        }
+      }
     }
     uint32_t v[E];
     uint32_t staged = ~0u;  // chunk whose twiddles are in shared memory (LSTAGE)
     for (uint32_t it = 0; t < t_end; t += t_step, ++it) {
-      const uint32_t buf = it & 1u;
+      const uint32_t buf = it % NS;
       uint32_t* cur = stage + buf * TWORDS;
-      const uint32_t tn = t + t_step;
+      const uint32_t tn = t + (NS - 1u) * t_step;  // the tile NS-1 ahead, into the buffer tile it-1 used
       if (tid == 0 && tn < t_end) {
-        tma::wait_reads();  // the store that last used the other buffer has read it
-        tma::mbar_expect_tx(&bar[buf ^ 1u], TBYTES);
-        tma_load(min, geo_run(a, tn), stage + (buf ^ 1u) * TWORDS, &bar[buf ^ 1u]);
+        const uint32_t nb = (it + NS - 1u) % NS;
+        tma::wait_reads();  // the store of tile it-1 (the last one issued) has read that buffer
+        tma::mbar_expect_tx(&bar[nb], TBYTES);
+        tma_load(min, geo_run(a, tn), stage + nb * TWORDS, &bar[nb]);
       }
       const Geo g = geo_run(a, t);
       if constexpr (LSTAGE) {
@@ -950,7 +973,7 @@ struct TPass {
       // the rounds in between touch only in-bounds shared memory and
       // twiddles whatever the tile holds, and every thread takes the same
       // barriers, so no extra CTA-wide barrier is needed per tile.
-      const bool ok = tma::mbar_wait(&bar[buf], (it >> 1) & 1u, kWaitNs);
+      const bool ok = tma::mbar_wait(&bar[buf], (it / NS) & 1u, kWaitNs);
       ld<kFirst>(cur, v, tid);
       if constexpr (DESC && TW) twist<kFirst>(v, a, g, tid);
       if constexpr (LSTAGE && KD == Kind::S)
@@ -963,7 +986,8 @@ struct TPass {
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(a.err, 1);
-          if (tn < t_end) tma::mbar_wait(&bar[buf ^ 1u], ((it + 1) >> 1) & 1u, kWaitNs);
+          for (uint32_t d = 1; d < NS; ++d)  // the loads in flight: tiles it+1 .. it+NS-1
+            if (t + d * t_step < t_end) tma::mbar_wait(&bar[(it + d) % NS], ((it + d) / NS) & 1u, kWaitNs);
           tma::wait_all();
         }
         return;

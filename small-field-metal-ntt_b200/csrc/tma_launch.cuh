@@ -126,7 +126,7 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     SFNTT_TRY(encode_s_map(&mout, r.out, r.lo, P, hb, 1ull << (r.lo + P), r.out_stride, r.batch));
     a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> (P + 5));
   }
-  constexpr int smem = 2 * (int)T::TBYTES + 32 + (int)T::SMEM_TW_BYTES + 1024;
+  constexpr int smem = T::kSmemBytes;
   auto kern = tma_pass_kernel<F, DESC, KD, P, PLAIN, TW, LSTAGE, HALVES>;
   static std::atomic<uint64_t> smem_done{0};
   SFNTT_TRY(smem_limit_once(kern, smem, ctx->device, smem_done));
