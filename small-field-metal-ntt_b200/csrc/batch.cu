@@ -144,7 +144,7 @@ Status prepare_item(sfntt_ctx* ctx, const sfntt_lde_item& it, cudaStream_t s) {
       if (lo > 12) {
         for (bool c12 : {false, true}) {
           uint32_t plo[4], pcnt[4];
-          const int k = tma_split(0, lo, plo, pcnt, c12);
+          const int k = tma_split(0, lo, plo, pcnt, c12, 14u);  // Montgomery fields
           for (int i = 1; i < k; ++i) {
             const bool compact = twist_compact_for(plo[i], pcnt[i]);
             SFNTT_TRY(monty_twist_table(ctx, f, plo[i], pcnt[i], true, s, &t, compact));

@@ -196,7 +196,7 @@ Status ntt_dev(sfntt_ctx* ctx, int field, int variant, bool inverse, uint32_t* d
 // column position & edge_mask -- the boundary with an adjacent strided pass
 // run by another kernel.
 // Layer split of a TMA range [a, b) (ntt.cu): passes lo[i], cnt[i]; 0 = none.
-int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first);
+int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first, uint32_t cmax);
 Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, uint32_t* out, uint64_t in_stride,
                   uint64_t out_stride, uint32_t log_n, uint32_t batch, uint32_t a, uint32_t b, uint32_t scale_w,
                   const uint2* tw, cudaStream_t stream, const uint2* edge_twist = nullptr,

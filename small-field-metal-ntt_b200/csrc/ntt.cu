@@ -14,11 +14,13 @@ namespace sfntt {
 
 // TMA plan for layers [0, b): one contiguous pass, then strided passes of at
 // most 8 layers.  Default: the strided passes take 8 layers each and the
-// contiguous pass the rest (5..13 layers: b = 13 and b = 21 need one pass
-// fewer than with at most 12).  c12_first (a tuning knob, for b > 12): the
+// contiguous pass the rest, 5..cmax layers (cmax 14 for the Montgomery fields:
+// b = 13, 14, 21, 22 then need one pass fewer than with at most 12; 13 for
+// M31, whose 14-layer pass reads its per-block twiddles -- twice its tile --
+// from L2 and was slower than 6 + 8 layers).  c12_first (a tuning knob, for b > 12): the
 // contiguous pass takes 12 layers and the strided passes share the rest as
 // evenly as possible (b = 14: 12 + 2 instead of 6 + 8).
-int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first) {
+int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first, uint32_t cmax) {
   if (a != 0) return 0;
   if (c12_first && b > 12) {
     const uint32_t s = (b - 12 + 7) / 8;
@@ -34,9 +36,9 @@ int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_
     }
     return (int)(1 + s);
   }
-  const uint32_t s = b > 13 ? (b - 13 + 7) / 8 : 0;
+  const uint32_t s = b > cmax ? (b - cmax + 7) / 8 : 0;
   const uint32_t c = b - 8 * s;
-  if (c < 5 || c > 13 || s > 3) return 0;
+  if (c < 5 || c > cmax || s > 3) return 0;
   lo[0] = 0;
   cnt[0] = c;
   for (uint32_t i = 1; i <= s; ++i) { lo[i] = c + 8 * (i - 1); cnt[i] = 8; }
@@ -73,7 +75,7 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
                   const uint2* tw, cudaStream_t s, const uint2* edge_twist, uint32_t edge_mask) {
   uint32_t lo[4], cnt[4];
   if (!ctx->no_tma) {
-    const int kt = tma_split(a, b, lo, cnt, ctx->split_c12);
+    const int kt = tma_split(a, b, lo, cnt, ctx->split_c12, is_monty(field) ? 14u : 13u);
     TmaRequest req[4];
     bool ok = kt > 0;
     for (int i = 0; i < kt && ok; ++i) {

@@ -43,8 +43,10 @@ constexpr bool kSwizzleC = true;
 // [c5 c6][c8 .. c11][c7][c12] instead -- bank (c0, c1, c2^c5, c3^c6, c4^c8),
 // conflict-free in every round -- by loading each half tile (c12 fixed)
 // through a 5-dimensional tensor map (32 words, rows c5..c6, rows c8 and up,
-// row c7, column).  Other layer counts are conflict-free in row order.
-__host__ __device__ constexpr bool c_row_perm(int P) { return P == 8 || P == 11 || P == 12; }
+// row c7, column).  The 14-layer pass's 2^14-word tiles keep the same low
+// rows, [c5 c6][c8 .. c12][c7][c13] (banks depend on c0 .. c8 alone).  Other
+// layer counts are conflict-free in row order.
+__host__ __device__ constexpr bool c_row_perm(int P) { return P == 8 || P == 11 || P == 12 || P == 14; }
 
 struct TmaArgs {
   const uint2* tw;     // twiddles (layer-concatenated Shoup pairs)
@@ -113,15 +115,18 @@ struct TPass {
   // is a layer bit above the lanes).  M31 contiguous tiles (any layer
   // count): the per-block twiddles of the tile's 2^13 positions.
   static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN && P == 8) ||
-                    (KD == Kind::C && !F::kMontgomery && !TW),
-                "position staging: BabyBear 8-layer strided or M31 contiguous tiles");
-  static constexpr int LT = (KD == Kind::C) ? (kTileBits - P) : 5;
+                    (KD == Kind::C && !F::kMontgomery && !TW && P <= kTileBits),
+                "position staging: BabyBear 8-layer strided or M31 contiguous 2^13-word tiles");
+  // Tile bits: 2^13-word tiles, except the 14-layer contiguous pass, whose
+  // tile is one 2^14-point group (64 KiB, 1024 threads, one CTA per SM).
+  static constexpr int TB = (KD == Kind::C && P > kTileBits) ? P : kTileBits;
+  static constexpr int LT = (KD == Kind::C) ? (TB - P) : 5;
   static constexpr int CB = P + LT;
   static constexpr int R = 4;
   static constexpr int NT = 1 << (CB - R);
   static constexpr int E = 1 << R;
   static constexpr int K = Plan<P, R>::K;
-  static_assert(KD == Kind::C ? CB == kTileBits : (P <= 8), "tile shape");
+  static_assert(KD == Kind::C ? (CB == TB && P <= 14) : (P <= 8), "tile shape");
   static constexpr uint32_t TWORDS = 1u << CB;
   static constexpr uint32_t TBYTES = 4u << CB;
 
@@ -207,7 +212,7 @@ struct TPass {
                                                 uint64_t* bar, bool whole) {
     if constexpr (kRowPerm) {
       tma::load_5d(dst, m, 0, 0, row >> 3, 0, col, bar);
-      if (whole) tma::load_5d(dst + TWORDS / 2, m, 0, 0, (row >> 3) + 16, 0, col, bar);
+      if (whole) tma::load_5d(dst + TWORDS / 2, m, 0, 0, (row >> 3) + (int32_t)(TWORDS / 512), 0, col, bar);
     } else {
       tma::load_3d(dst, m, 0, row, col, bar);
     }
@@ -216,7 +221,7 @@ struct TPass {
                                                  bool whole) {
     if constexpr (kRowPerm) {
       tma::store_5d(m, 0, 0, row >> 3, 0, col, src);
-      if (whole) tma::store_5d(m, 0, 0, (row >> 3) + 16, 0, col, src + TWORDS / 2);
+      if (whole) tma::store_5d(m, 0, 0, (row >> 3) + (int32_t)(TWORDS / 512), 0, col, src + TWORDS / 2);
     } else {
       tma::store_3d(m, 0, row, col, src);
     }
@@ -233,8 +238,8 @@ struct TPass {
   // 16 t .. 16 t + 15 (four layers, thread bits 4..12 in order) read that
   // round's per-block twiddles from the table's first-round copy (TmaArgs::tw0).
   static constexpr bool round0_linear() {
-    const RoundMap mp = make_map<KD, P, (KD == Kind::C) ? (kTileBits - P) : 5, 4>(0);
-    return Plan<P, 4>::r(0) == 4 && mp.mpos[0] == 0 && mp.mpos[1] == 1 && mp.mpos[2] == 2 && mp.mpos[3] == 3 &&
+    const RoundMap mp = make_map<KD, P, LT, 4>(0);
+    return CB == kTileBits && Plan<P, 4>::r(0) == 4 && mp.mpos[0] == 0 && mp.mpos[1] == 1 && mp.mpos[2] == 2 && mp.mpos[3] == 3 &&
            mp.ngrp == 1 && mp.gshift[0] == 4 && mp.gmask[0] == (1u << (kTileBits - 4)) - 1u;
   }
   static constexpr bool kRound0Copy = !F::kMontgomery && KD == Kind::C && round0_linear();
@@ -260,7 +265,7 @@ struct TPass {
   // staged twiddle bytes in shared memory, CTAs per SM
   static constexpr uint32_t SMEM_TW_BYTES =
       LSTAGE ? (KD == Kind::S ? 2u * 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
-  static constexpr int kCtasPerSm = (LSTAGE && KD == Kind::S) ? 1 : 2;
+  static constexpr int kCtasPerSm = ((LSTAGE && KD == Kind::S) || NT > 512) ? 1 : 2;
   // Tile buffers of the whole-tile pipeline (run): three -- the tiles two and
   // one ahead in flight while one is computed -- for the staged strided passes
   // (one CTA per SM, 227 KiB with the twiddle chunks: 2^20 x 256 natural-order
@@ -497,7 +502,9 @@ struct TPass {
   static constexpr bool kSwz = (KD == Kind::C) && kSwizzleC;
   static constexpr bool kRowPerm = (KD == Kind::C) && c_row_perm(P);
   __host__ __device__ static constexpr uint32_t lay(uint32_t c) {
-    return kRowPerm ? ((c & ~0xF80u) | ((c >> 1) & 0x780u) | ((c & 0x80u) << 4)) : c;
+    // rows [c5 c6][c8 .. c(TB-2)][c7][c(TB-1)]
+    constexpr uint32_t MID = ((1u << (TB - 1)) - 1u) & ~0x7Fu;  // c7 .. c(TB-2)
+    return kRowPerm ? ((c & ~MID) | ((c >> 1) & (MID >> 1) & ~0x7Fu) | ((c & 0x80u) << (TB - 9))) : c;
   }
   __host__ __device__ static constexpr uint32_t sw(uint32_t c) {
     const uint32_t s = lay(c);

@@ -45,7 +45,7 @@ inline bool tma_pass_ok(const TmaRequest& r) {
   if (!aligned16(r.in) || !aligned16(r.out) || (r.in_stride & 3) || (r.out_stride & 3)) return false;
   const uint64_t n = 1ull << r.log_n;
   if (r.contiguous) {
-    if (r.P < 5 || r.P > 13 || r.lo != 0) return false;
+    if (r.P < 5 || r.P > 14 || r.lo != 0) return false;
     if (n >= kTileWords) return true;
     return r.in_stride == n && r.out_stride == n && ((uint64_t)r.batch * n) % kTileWords == 0;
   }
@@ -66,9 +66,11 @@ inline Status encode_c_map(CUtensorMap* m, const uint32_t* base, uint32_t log_n,
   const uint64_t cols = n >= kTileWords ? batch : 1;
   const uint64_t col_bytes = n >= kTileWords ? stride * 4 : (uint64_t)batch * n * 4;
   if (c_row_perm(P)) {
+    // half a tile per copy: 2^(tile bits - 1) words; 14-layer passes have 2^14-word tiles
+    const uint32_t half_words = (P > (int)kTileBits ? (1u << P) : kTileWords) / 2;
     const cuuint64_t dims[5] = {32, 4, rows / 8, 2, cols};
     const cuuint64_t strides[4] = {128, 1024, 512, col_bytes};
-    const cuuint32_t box[5] = {32, 4, kTileWords / 32 / 16, 2, 1};
+    const cuuint32_t box[5] = {32, 4, half_words / 256, 2, 1};
     return tensor_map_encode(m, base, 5, dims, strides, box, kSwizzleC);
   }
   const cuuint64_t dims[3] = {32, rows, cols};
@@ -112,14 +114,14 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
   a.twist_mask = r.twist_mask;
   a.twist_compact = r.twist_compact ? 1u : 0u;
   if constexpr (KD == Kind::C) {
-    const uint32_t rows = HALVES ? T::HROWS : kTileWords / 32;
+    const uint32_t rows = HALVES ? T::HROWS : T::TWORDS / 32;
     SFNTT_TRY(encode_c_map(&min, r.in, r.log_n, r.in_stride, r.batch, P, rows));
     SFNTT_TRY(encode_c_map(&mout, r.out, r.log_n, r.out_stride, r.batch, P, rows));
-    a.spans = n < kTileWords;
-    a.log_tpc = a.spans ? 0u : r.log_n - kTileBits;
+    a.spans = n < T::TWORDS;
+    a.log_tpc = a.spans ? 0u : r.log_n - T::CB;
     // every M31 table with n >= 2^13 carries its first-round copy from entry n on
     if constexpr (T::kRound0Copy) a.tw0 = a.spans ? nullptr : r.tw + n;
-    a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> kTileBits);
+    a.ntiles = (uint32_t)(((uint64_t)r.batch * n) >> T::CB);
   } else {
     const uint64_t hb = n >> (r.lo + P);
     SFNTT_TRY(encode_s_map(&min, r.in, r.lo, P, hb, 1ull << (r.lo + P), r.in_stride, r.batch));
@@ -148,8 +150,9 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
         return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);                    \
       }                                                                                          \
     } else {                                                                                     \
-      if (r.lstage && r.log_n >= kTileBits)                                                      \
-        return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);             \
+      if constexpr (PP <= (int)kTileBits)                                                        \
+        if (r.lstage && r.log_n >= kTileBits)                                                    \
+          return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);           \
     }                                                                                            \
     if constexpr (TPass<F, DESC, Kind::C, PP, false, false>::halves_ok())                        \
       if (ctx->c_halves) return launch_tma_pass<F, DESC, Kind::C, PP, false, false, false, true>(ctx, r, s); \
@@ -174,6 +177,7 @@ Status run_tma_pass_impl(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
     switch (r.P) {
       SFNTT_TMA_C(5) SFNTT_TMA_C(6) SFNTT_TMA_C(7) SFNTT_TMA_C(8)
       SFNTT_TMA_C(9) SFNTT_TMA_C(10) SFNTT_TMA_C(11) SFNTT_TMA_C(12) SFNTT_TMA_C(13)
+      SFNTT_TMA_C(14)
       default: break;
     }
   } else {

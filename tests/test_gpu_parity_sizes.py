@@ -142,8 +142,10 @@ def _m31_batch(fn, x, log_n, batch):
     return np.concatenate([fn(x[c * n:(c + 1) * n]) for c in range(batch)])
 
 
-@pytest.mark.parametrize("log_n,batch", [(13, 3), (21, 2)])
+@pytest.mark.parametrize("log_n,batch", [(13, 3), (21, 2), (14, 160), (22, 2)])
 def test_thirteen_layer_batches(ctx, log_n, batch):
+    """13- and 14-layer contiguous passes: 2^13 and 2^21 (13 + 8), 2^14 past
+    one cluster wave and 2^22 (14 + 8: the 2^14-word tiles of 1024 threads)."""
     import torch
     n = 1 << log_n
     xb = O.lcg(batch * n, 1300 + log_n, O.BB_P, monty=True)
@@ -163,11 +165,12 @@ def test_thirteen_layer_batches(ctx, log_n, batch):
         assert np.array_equal(d.cpu().numpy().view(np.uint32), inv(x)), log_n
 
 
-@pytest.mark.parametrize("batch", [2, 16])
-def test_lde_log_n_21(ctx, batch):
-    """BabyBear coset LDE and M31 blow-up at 2^21 (low layers: one 13-layer
-    contiguous pass each way); 16 columns take the M31 staged-twiddle passes."""
-    log_n, added = 21, 1
+@pytest.mark.parametrize("log_n,batch", [(21, 2), (21, 16), (22, 2), (22, 16)])
+def test_lde_log_n_21_22(ctx, log_n, batch):
+    """BabyBear coset LDE and M31 blow-up at 2^21 and 2^22 (low layers: one
+    13- or 14-layer contiguous pass each way); 16 columns take the M31
+    staged-twiddle passes at 2^21 (the 14-layer pass reads them from L2)."""
+    added = 1
     xb = O.lcg(batch << log_n, 2100 + batch, O.BB_P, monty=True)
     r = sfntt.CosetLdeBatch(ctx).execute(xb, log_n, batch, added)
     assert np.array_equal(r.data, O.bb_coset_lde(xb, log_n, batch, added, threads=8))
