@@ -15,9 +15,10 @@ namespace sfntt {
 // TMA plan for layers [0, b): one contiguous pass, then strided passes of at
 // most 8 layers.  Default: the strided passes take 8 layers each and the
 // contiguous pass the rest, 5..cmax layers (cmax 14 for the Montgomery fields:
-// b = 13, 14, 21, 22 then need one pass fewer than with at most 12; 13 for
-// M31, whose 14-layer pass reads its per-block twiddles -- twice its tile --
-// from L2 and was slower than 6 + 8 layers).  c12_first (a tuning knob, for b > 12): the
+// b = 13, 14, 21, 22 then need one pass fewer than with at most 12; for M31
+// where its contiguous passes stage their per-block twiddles, 13 elsewhere:
+// reading them from L2 -- twice the tile -- the 14-layer pass was slower than
+// 6 + 8 layers).  c12_first (a tuning knob, for b > 12): the
 // contiguous pass takes 12 layers and the strided passes share the rest as
 // evenly as possible (b = 14: 12 + 2 instead of 6 + 8).
 int tma_split(uint32_t a, uint32_t b, uint32_t lo[4], uint32_t cnt[4], bool c12_first, uint32_t cmax) {
@@ -75,7 +76,9 @@ Status layers_dev(sfntt_ctx* ctx, int field, bool inverse, const uint32_t* in, u
                   const uint2* tw, cudaStream_t s, const uint2* edge_twist, uint32_t edge_mask) {
   uint32_t lo[4], cnt[4];
   if (!ctx->no_tma) {
-    const int kt = tma_split(a, b, lo, cnt, ctx->split_c12, is_monty(field) ? 14u : 13u);
+    // M31 takes the 14-layer pass only where it stages its per-block twiddles (16 or more columns)
+    const uint32_t cmax = (is_monty(field) || (log_n >= 13 && batch >= 16)) ? 14u : 13u;
+    const int kt = tma_split(a, b, lo, cnt, ctx->split_c12, cmax);
     TmaRequest req[4];
     bool ok = kt > 0;
     for (int i = 0; i < kt && ok; ++i) {

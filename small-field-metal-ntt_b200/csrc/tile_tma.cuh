@@ -115,8 +115,8 @@ struct TPass {
   // is a layer bit above the lanes).  M31 contiguous tiles (any layer
   // count): the per-block twiddles of the tile's 2^13 positions.
   static_assert(!LSTAGE || (KD == Kind::S && F::kMontgomery && !PLAIN && P == 8) ||
-                    (KD == Kind::C && !F::kMontgomery && !TW && P <= kTileBits),
-                "position staging: BabyBear 8-layer strided or M31 contiguous 2^13-word tiles");
+                    (KD == Kind::C && !F::kMontgomery && !TW),
+                "position staging: BabyBear 8-layer strided or M31 contiguous tiles");
   // Tile bits: 2^13-word tiles, except the 14-layer contiguous pass, whose
   // tile is one 2^14-point group (64 KiB, 1024 threads, one CTA per SM).
   static constexpr int TB = (KD == Kind::C && P > kTileBits) ? P : kTileBits;
@@ -264,7 +264,7 @@ struct TPass {
   static constexpr uint32_t CTILE_ENTRIES = 8190u;
   // staged twiddle bytes in shared memory, CTAs per SM
   static constexpr uint32_t SMEM_TW_BYTES =
-      LSTAGE ? (KD == Kind::S ? 2u * 8u * 32u * ((1u << P) - 1u) : 4u * 8192u) : 8u * TW_ENTRIES;
+      LSTAGE ? (KD == Kind::S ? 2u * 8u * 32u * ((1u << P) - 1u) : 4u * TWORDS) : 8u * TW_ENTRIES;
   static constexpr int kCtasPerSm = ((LSTAGE && KD == Kind::S) || NT > 512) ? 1 : 2;
   // Tile buffers of the whole-tile pipeline (run): three -- the tiles two and
   // one ahead in flight while one is computed -- for the staged strided passes
@@ -323,7 +323,7 @@ struct TPass {
       return tws[32u * em + ((((ct >> 5) & em) + ((cm >> 5) & em)) << 5) + (ct & 31u)];
     } else if constexpr (LSTAGE && KD == Kind::C) {  // M31: the tile's staged table-order copy (w' = 2w + (w >> 30))
       static_assert(!kStageThreadOrder, "12-layer rounds take their staged twiddles in round()");
-      const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (8192u - (8192u >> L));
+      const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (TWORDS - (TWORDS >> L));
       const uint32_t ws = tw32[(ct >> (L + 1)) + (cm >> (L + 1))];
       return make_uint2(ws >> 1, ws);
     } else if constexpr (F::kMontgomery) {  // BabyBear strided, per position: tw[L][pos mod 2^L]
@@ -364,7 +364,7 @@ struct TPass {
         uint2 tv[E / 2];
         if constexpr (LSTAGE) {
           // this thread's 2^(r-1-j) twiddles of layer j (a constant once unrolled)
-          const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (8192u - (8192u >> L));
+          const uint32_t* tw32 = reinterpret_cast<const uint32_t*>(tws) + (TWORDS - (TWORDS >> L));
           if constexpr (k == 0 && kStageThreadOrder) {  // thread-ordered first-round layers
             switch (r - 1 - j) {
               case 3: staged_w<4, 0>(tw32 + 4u * tid, tv); staged_w<4, 4>(tw32 + 4u * (NT + tid), tv); break;
@@ -815,15 +815,16 @@ struct TPass {
   static constexpr uint32_t HWORDS = TWORDS / 2, HBYTES = TBYTES / 2, HROWS = HWORDS / 32;
 
   // M31 per-block twiddles (Shoup companions) of every layer L < P over tile
-  // positions [pos_base, pos_base + 2^13), all in table order: 2^(12-L)
-  // consecutive entries of layer L at 8192 - (8192 >> L).
+  // positions [pos_base, pos_base + 2^CB), all in table order: 2^(CB-1-L)
+  // consecutive entries of layer L at 2^CB - (2^CB >> L).
   __device__ static __forceinline__ void stage_ctile_plain(uint32_t* dst, const TmaArgs& a, uint32_t pos_base,
                                                            uint32_t tid) {
     const uint32_t n = 1u << a.log_n;
-    const uint32_t end = 8192u - (8192u >> P);
+    const uint32_t end = TWORDS - (TWORDS >> P);
     for (uint32_t e = tid; e < end; e += NT) {
-      const uint32_t L = 12u - (31u - __clz(8191u - e));  // e in [8192 - 2^(13-L), 8192 - 2^(12-L))
-      const uint32_t local = e - (8192u - (8192u >> L));
+      // e in [2^CB - 2^(CB-L), 2^CB - 2^(CB-1-L))
+      const uint32_t L = (uint32_t)(CB - 1) - (31u - __clz(TWORDS - 1u - e));
+      const uint32_t local = e - (TWORDS - (TWORDS >> L));
       dst[e] = __ldg(&a.tw[(n - (n >> L)) + (pos_base >> (L + 1)) + local].y);
     }
   }

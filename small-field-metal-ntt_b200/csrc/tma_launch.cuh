@@ -150,9 +150,8 @@ Status launch_tma_pass(sfntt_ctx* ctx, const TmaRequest& r, cudaStream_t s) {
         return launch_tma_pass<F, DESC, Kind::C, PP, false, true>(ctx, r, s);                    \
       }                                                                                          \
     } else {                                                                                     \
-      if constexpr (PP <= (int)kTileBits)                                                        \
-        if (r.lstage && r.log_n >= kTileBits)                                                    \
-          return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);           \
+      if (r.lstage && r.log_n >= kTileBits)                                                      \
+        return launch_tma_pass<F, DESC, Kind::C, PP, false, false, true>(ctx, r, s);             \
     }                                                                                            \
     if constexpr (TPass<F, DESC, Kind::C, PP, false, false>::halves_ok())                        \
       if (ctx->c_halves) return launch_tma_pass<F, DESC, Kind::C, PP, false, false, false, true>(ctx, r, s); \
