@@ -79,6 +79,19 @@ __host__ __device__ constexpr RoundMap make_map(int k) {
     used[EOFF + b + j] = true;
   }
   int f = r;
+  // 14-layer contiguous tiles (one 2^14-point group, rounds of 4, 4, 3, 3
+  // layers): fillers c11 (third round) and c7 (fourth) keep the thread bits
+  // that two consecutive rounds share on the same thread-id bits, so their
+  // exchanges group the warps (4 groups each) instead of taking the whole
+  // 1024-thread CTA (with the highest free bits, c13 and c10, the second
+  // exchange is CTA-wide); every round stays bank-conflict-free.
+  if (KD == Kind::C && P == 14 && LT == 0 && R == 4 && f < R && (k == 2 || k == 3)) {
+    const int c = k == 2 ? 11 : 7;
+    if (!used[c]) {
+      m.mpos[f++] = c;
+      used[c] = true;
+    }
+  }
   for (int c = CB - 1; c >= 0 && f < R; --c) {
     if (!used[c]) {
       m.mpos[f++] = c;

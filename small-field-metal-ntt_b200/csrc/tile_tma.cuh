@@ -1019,6 +1019,11 @@ static_assert(TPass<BabyBear, false, Kind::C, 12>::shfl_swap(0, 1) && TPass<Baby
                   TPass<BabyBear, false, Kind::C, 8>::shfl_swap(0, 1) && !TPass<BabyBear, false, Kind::C, 12>::shfl_swap(1, 2) &&
                   !TPass<BabyBear, false, Kind::S, 8>::shfl_swap(0, 1),
               "warp-local exchanges of the shuffle form");
+// 14-layer passes: a warp-local exchange, then two grouped ones (4 groups each)
+static_assert(TPass<BabyBear, false, Kind::C, 14>::xgroups(0, 1) == 0 && TPass<BabyBear, false, Kind::C, 14>::xgroups(1, 2) == 4 &&
+                  TPass<BabyBear, false, Kind::C, 14>::xgroups(2, 3) == 4 && TPass<BabyBear, false, Kind::C, 14>::xbase(3) == 5 &&
+                  TPass<BabyBear, false, Kind::C, 14>::xfixed<0, 1>() >= 0,
+              "C14 exchanges: warp, 4 groups, 4 groups");
 // 13-layer passes: two grouped exchanges in a row (4 groups each), on disjoint ids
 static_assert(TPass<BabyBear, false, Kind::C, 13>::xgroups(1, 2) == 4 && TPass<BabyBear, false, Kind::C, 13>::xgroups(2, 3) == 4 &&
                   TPass<BabyBear, false, Kind::C, 13>::xbase(3) == 5 && TPass<BabyBear, true, Kind::C, 13>::xbase(2) == 5,
