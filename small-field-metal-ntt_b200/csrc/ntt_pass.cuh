@@ -66,6 +66,28 @@ struct RoundMap {
   int gshift[16];
 };
 
+// Filler bits: the tile bits of round k's slot bits r .. R-1 (i = 0, 1, ...),
+// -1 = the highest free tile bits.  A search over the choices (against each
+// round's thread map and the shared-memory bank model) looked for fillers that
+// keep the thread bits two consecutive rounds share on the same thread-id bits
+// -- so the exchange groups the warps instead of taking the whole CTA -- with
+// no more bank conflicts.  Kept where it measured faster:
+//   11 layers (rounds 4, 4, 3):            - | - | c11   CTA -> 2 groups; tile bit 12
+//     then stays on thread bit 8 in every round: independent halves (2^19 x 64
+//     forward + inverse 298 -> 292 us, 2^19 x 128 LDE 0.820 -> 0.804 ms)
+//   14 layers (4, 4, 3, 3; 2^14-word tiles): - | - | c11 | c7   CTA + 8 groups
+//     -> 4 + 4 groups (2^22 x 64 LDE 3.81 -> 3.77 ms)
+// Dropped: 9 layers, c7 | c8 | c2 (both exchanges warp-local) made the twisted
+// 9-layer pass 6 % slower -- its lanes then span tile bits 0, 1, 3, 4, 5 and the
+// twist's global loads twice the sectors; 5 layers (CTA -> warp): no change.
+template <Kind KD, int P, int LT, int R>
+__host__ __device__ constexpr int filler_hint(int k, int i) {
+  if (KD != Kind::C || R != 4 || i != 0) return -1;
+  if (P == 14 && LT == 0) return k == 2 ? 11 : k == 3 ? 7 : -1;
+  if (P == 11 && LT == 2) return k == 2 ? 11 : -1;
+  return -1;
+}
+
 template <Kind KD, int P, int LT, int R>
 __host__ __device__ constexpr RoundMap make_map(int k) {
   constexpr int CB = P + LT;
@@ -79,18 +101,11 @@ __host__ __device__ constexpr RoundMap make_map(int k) {
     used[EOFF + b + j] = true;
   }
   int f = r;
-  // 14-layer contiguous tiles (one 2^14-point group, rounds of 4, 4, 3, 3
-  // layers): fillers c11 (third round) and c7 (fourth) keep the thread bits
-  // that two consecutive rounds share on the same thread-id bits, so their
-  // exchanges group the warps (4 groups each) instead of taking the whole
-  // 1024-thread CTA (with the highest free bits, c13 and c10, the second
-  // exchange is CTA-wide); every round stays bank-conflict-free.
-  if (KD == Kind::C && P == 14 && LT == 0 && R == 4 && f < R && (k == 2 || k == 3)) {
-    const int c = k == 2 ? 11 : 7;
-    if (!used[c]) {
-      m.mpos[f++] = c;
-      used[c] = true;
-    }
+  for (int i = 0; f < R; ++i) {
+    const int c = filler_hint<KD, P, LT, R>(k, i);
+    if (c < 0 || used[c]) break;
+    m.mpos[f++] = c;
+    used[c] = true;
   }
   for (int c = CB - 1; c >= 0 && f < R; --c) {
     if (!used[c]) {

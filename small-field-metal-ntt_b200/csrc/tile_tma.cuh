@@ -1019,6 +1019,9 @@ static_assert(TPass<BabyBear, false, Kind::C, 12>::shfl_swap(0, 1) && TPass<Baby
                   TPass<BabyBear, false, Kind::C, 8>::shfl_swap(0, 1) && !TPass<BabyBear, false, Kind::C, 12>::shfl_swap(1, 2) &&
                   !TPass<BabyBear, false, Kind::S, 8>::shfl_swap(0, 1),
               "warp-local exchanges of the shuffle form");
+// the 11-layer pass's filler (see filler_hint): a grouped exchange and independent halves
+static_assert(TPass<BabyBear, false, Kind::C, 11>::xgroups(1, 2) == 2 && TPass<BabyBear, false, Kind::C, 11>::halves_ok(),
+              "filler choice of the 11-layer pass");
 // 14-layer passes: a warp-local exchange, then two grouped ones (4 groups each)
 static_assert(TPass<BabyBear, false, Kind::C, 14>::xgroups(0, 1) == 0 && TPass<BabyBear, false, Kind::C, 14>::xgroups(1, 2) == 4 &&
                   TPass<BabyBear, false, Kind::C, 14>::xgroups(2, 3) == 4 && TPass<BabyBear, false, Kind::C, 14>::xbase(3) == 5 &&
