@@ -459,13 +459,13 @@ def step_stats(ms: list) -> dict:
 
 def headline_keys(secondary, uneven, served) -> dict:
     """The other configurations' headline numbers as top-level scalars:
-    the M31 2^16 forward + inverse pair, the BabyBear 2^20 and 2^24 pairs, the
+    the M31 2^16 forward + inverse pair, the BabyBear 2^10..2^24 pairs, the
     uneven batch (plain loop and one launch) and the served stream at its
     highest rate."""
     out = {}
     if secondary:
         out["m31_2^16_fwd_inv_us"] = secondary["m31"]["16"]["fwd_inv_us"]
-        for k in ("10", "16", "20", "24"):
+        for k in ("10", "16", "20", "21", "22", "24"):
             out[f"bb_2^{k}_fwd_inv_us"] = secondary["bb"][k]["fwd_inv_us"]
         out["bb_2^24_gelem_s"] = secondary["bb"]["24"]["gelem_s"]
     if uneven:
